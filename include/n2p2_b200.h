@@ -1,0 +1,172 @@
+/*
+ * n2p2_b200 — C-ABI of the B200 implementation of n2p2's 2G-HDNNP
+ * prediction path (neighbor list, symmetry functions + derivatives, atomic
+ * neural networks, energy, forces).
+ *
+ * Every entry point returns an int status (0 = success, negative = error) and
+ * never throws; n2p2b_last_error() returns the message of the last failure
+ * on a context.  The n2p2 C++ API reports the same conditions with
+ * std::runtime_error / std::range_error / std::out_of_range; the C++ and
+ * Python shims re-raise them.
+ *
+ * Units: positions, box and results are in the potential's PHYSICAL units
+ * (those of input.data).  If input.nn normalizes (mean_energy, conv_energy,
+ * conv_length) the conversion happens inside, exactly as
+ * Prediction::readStructureFromFile / Prediction::predict do it.
+ * Intermediate arrays (G, dE/dG, dG/dr, neighbor displacements) are returned
+ * in the normalized units the reference holds them in during evaluateNNP.
+ *
+ * Threading: a context is used by one host thread at a time (as nnp::Mode).
+ * All device work of a context runs in order on one CUDA stream.
+ */
+#ifndef N2P2_B200_H
+#define N2P2_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct n2p2b_context n2p2b_context;
+
+/* Status codes. */
+#define N2P2B_OK                 0
+#define N2P2B_ERR_ARGUMENT      -1  /* invalid argument                      */
+#define N2P2B_ERR_SETUP         -2  /* input.nn / scaling / weights problem  */
+#define N2P2B_ERR_CUDA          -3  /* CUDA runtime error                    */
+#define N2P2B_ERR_CAPACITY      -4  /* capacity exceeded and not recoverable */
+#define N2P2B_ERR_STATE         -5  /* call out of order (no setup/structure)*/
+#define N2P2B_ERR_INTERNAL      -6  /* broken invariant (reported, not hit)  */
+
+/* Where an array argument lives. */
+#define N2P2B_HOST               0
+#define N2P2B_DEVICE             1
+
+/* n2p2b_set_structure flags. */
+#define N2P2B_REMAP              1  /* wrap periodic positions into the cell
+                                       (Structure::remap, as readFromLines) */
+
+/* ---- context ---------------------------------------------------------- */
+
+/* Creates a context on CUDA device `device`.  Replaces constructing
+ * nnp::Mode / nnp::Prediction (libnnp/Mode.h:86, Prediction.h:27). */
+int         n2p2b_create(int device, n2p2b_context** ctx);
+void        n2p2b_destroy(n2p2b_context* ctx);
+const char* n2p2b_last_error(const n2p2b_context* ctx);
+/* Runs the context's device work on `stream` (a cudaStream_t, NULL = own). */
+int         n2p2b_set_stream(n2p2b_context* ctx, void* stream);
+
+/* ---- setup (nnp::Mode / nnp::Prediction) ------------------------------ */
+
+/* Mode::loadSettingsFile (libnnp/Mode.cpp:161-210). */
+int n2p2b_load_settings_file(n2p2b_context* ctx, const char* path);
+/* Mode::setupGeneric (libnnp/Mode.cpp:212-236): normalization, elements,
+ * cutoff, symmetry functions, dG/dr slot tables, SF groups, NN topology.
+ * Includes Mode::setupSymmetryFunctionGroups (libnnp/Mode.cpp:842-892). */
+int n2p2b_setup_generic(n2p2b_context* ctx);
+/* Mode::setupSymmetryFunctionScaling (libnnp/Mode.cpp:712-840); path NULL
+ * = Mode::setupSymmetryFunctionScalingNone. */
+int n2p2b_setup_symmetry_function_scaling(n2p2b_context* ctx,
+                                          const char* path);
+/* Mode::setupNeuralNetworkWeights (libnnp/Mode.cpp:1451-1478); format is a
+ * printf pattern taking the atomic number, e.g. "dir/weights.%03zu.data". */
+int n2p2b_setup_neural_network_weights(n2p2b_context* ctx,
+                                       const char* format);
+/* Prediction::setup (libnnp/Prediction.cpp:34-46) on a potential directory
+ * holding input.nn, scaling.data and weights.%03zu.data. */
+int n2p2b_setup(n2p2b_context* ctx, const char* directory);
+
+/* ---- potential queries ------------------------------------------------ */
+
+int    n2p2b_num_elements(const n2p2b_context* ctx);
+/* Element symbol of element index e (element order = n2p2's ElementMap). */
+int    n2p2b_element_symbol(const n2p2b_context* ctx, int e, char* buf,
+                            size_t len);
+int    n2p2b_element_index(const n2p2b_context* ctx, const char* symbol);
+/* Element::numSymmetryFunctions. */
+int    n2p2b_num_symmetry_functions(const n2p2b_context* ctx, int e);
+/* Element::getSymmetryFunctionNumTable()[ne] (libnnp/Element.cpp:289-311). */
+int    n2p2b_num_slots(const n2p2b_context* ctx, int e, int ne);
+/* Mode::getMaxCutoffRadius (normalized units, libnnp/Mode.h:693). */
+double n2p2b_max_cutoff_radius(const n2p2b_context* ctx);
+
+/* ---- structure (nnp::Structure) --------------------------------------- */
+
+/* Sets the atoms to evaluate: Structure::readFromLines's data
+ * (libnnp/Structure.cpp:142-271) without text parsing.  box: 9 doubles,
+ * box[3k+c] = component c of lattice vector k, or NULL for a non-periodic
+ * structure.  positions: num_atoms x 3 (physical units), host or device.
+ * elements: num_atoms element indices (host).  flags: N2P2B_REMAP. */
+int n2p2b_set_structure(n2p2b_context* ctx, int64_t num_atoms,
+                        const double* box, const double* positions,
+                        int positions_location, const int32_t* elements,
+                        int flags);
+/* New coordinates for the current atoms (next frame / MD step). */
+int n2p2b_set_positions(n2p2b_context* ctx, const double* positions,
+                        int positions_location);
+
+/* ---- evaluation steps (nnp::Mode) ------------------------------------- */
+
+/* Structure::calculateNeighborList(getMaxCutoffRadius(), false)
+ * (libnnp/Structure.cpp:287-399). */
+int n2p2b_calculate_neighbor_list(n2p2b_context* ctx);
+/* Mode::calculateSymmetryFunctionGroups (libnnp/Mode.cpp:1561-1640). */
+int n2p2b_calculate_symmetry_function_groups(n2p2b_context* ctx,
+                                             int derivatives);
+/* Mode::calculateAtomicNeuralNetworks (libnnp/Mode.cpp:1642-1751). */
+int n2p2b_calculate_atomic_neural_networks(n2p2b_context* ctx,
+                                           int derivatives);
+/* Mode::calculateEnergy (libnnp/Mode.cpp:1803-1828). */
+int n2p2b_calculate_energy(n2p2b_context* ctx);
+/* Mode::calculateForces (libnnp/Mode.cpp:1849-1912). */
+int n2p2b_calculate_forces(n2p2b_context* ctx);
+/* Mode::evaluateNNP (libnnp/Mode.cpp:1967-2016) followed by the physical
+ * unit conversion and energy offsets of Prediction::predict
+ * (libnnp/Prediction.cpp:65-76). */
+int n2p2b_evaluate(n2p2b_context* ctx, int use_forces);
+/* Enqueues the whole evaluation on the context's stream without any host
+ * synchronization (capacities must already fit, e.g. after one
+ * n2p2b_evaluate on a structure of the same size).  Check the outcome with
+ * n2p2b_finish. */
+int n2p2b_evaluate_async(n2p2b_context* ctx, int use_forces);
+/* Waits for the context's stream and reports capacity / invariant flags. */
+int n2p2b_finish(n2p2b_context* ctx);
+
+/* ---- results ---------------------------------------------------------- */
+
+/* Structure::energy after Prediction::predict (physical units, offsets). */
+int n2p2b_get_energy(n2p2b_context* ctx, double* energy);
+/* Atom::f after Prediction::predict: num_atoms x 3, physical units. */
+int n2p2b_get_forces(n2p2b_context* ctx, double* forces, int location);
+/* Atom::energy after Prediction::predict (physical units, no offsets). */
+int n2p2b_get_atomic_energies(n2p2b_context* ctx, double* energies);
+/* Atom::numNeighbors per atom. */
+int n2p2b_get_neighbor_counts(n2p2b_context* ctx, int64_t* counts);
+/* Atom::neighbors (index, dr, d) concatenated per atom, in the reference's
+ * list order (j ascending, then image). */
+int n2p2b_get_neighbor_list(n2p2b_context* ctx, int64_t* index, double* dr,
+                            double* d);
+/* Atom::G / Atom::dEdG as [atom][stride]. */
+int n2p2b_get_symmetry_functions(n2p2b_context* ctx, double* G, int stride);
+int n2p2b_get_dEdG(n2p2b_context* ctx, double* dEdG, int stride);
+/* Atom::dGdr ([atom][sf_stride][3]) and Neighbor::dGdr ([entry][slot_stride]
+ * [3], entries in n2p2b_get_neighbor_list order). */
+int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sf_stride,
+                   double* neighbor, int slot_stride);
+
+/* ---- one call per frame ----------------------------------------------- */
+
+/* Prediction::readStructureFromFile + Prediction::predict on in-memory
+ * host arrays: sets the structure (with remap), evaluates, copies energy and
+ * forces (num_atoms x 3) back to the host. */
+int n2p2b_predict(n2p2b_context* ctx, int64_t num_atoms, const double* box,
+                  const double* positions, const int32_t* elements,
+                  double* energy, double* forces);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* N2P2_B200_H */

@@ -1,0 +1,1340 @@
+// Context: owns the potential, the device tables and the device buffers of
+// one structure, and runs the prediction pipeline behind the C-ABI
+// (include/n2p2_b200.h).  Host-side geometry (inverse box, periodic image
+// counts) is computed with the reference's own expressions; this file is
+// compiled with -ffp-contract=off for its host code so those roundings match.
+#include "n2p2_b200.h"
+
+#include "kernels.h"
+#include "potential.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <exception>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+using namespace n2p2b;
+
+namespace
+{
+
+struct CudaError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+struct CapacityError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+struct StateError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+void ck(cudaError_t e, char const* what)
+{
+    if (e != cudaSuccess)
+    {
+        throw CudaError(std::string("CUDA error in ") + what + ": "
+                        + cudaGetErrorString(e));
+    }
+}
+
+// Grow-only device allocation.
+struct DevBuf
+{
+    void*       p = nullptr;
+    std::size_t bytes = 0;
+    void ensure(std::size_t b)
+    {
+        if (b <= bytes && p != nullptr) return;
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+        std::size_t const want = std::max<std::size_t>(b, 256);
+        ck(cudaMalloc(&p, want), "cudaMalloc");
+        bytes = want;
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
+// --- reference geometry (libnnp/Vec3D.h, Structure.cpp) --------------------
+
+struct V3
+{
+    double r[3];
+};
+
+V3 cross(V3 const& a, V3 const& b)
+{
+    V3 w;
+    w.r[0] = a.r[1] * b.r[2] - a.r[2] * b.r[1];
+    w.r[1] = a.r[2] * b.r[0] - a.r[0] * b.r[2];
+    w.r[2] = a.r[0] * b.r[1] - a.r[1] * b.r[0];
+    return w;
+}
+
+V3 normalized(V3 v)
+{
+    double const n = std::sqrt(v.r[0] * v.r[0] + v.r[1] * v.r[1]
+                               + v.r[2] * v.r[2]);
+    v.r[0] /= n;
+    v.r[1] /= n;
+    v.r[2] /= n;
+    return v;
+}
+
+double dot(V3 const& a, V3 const& b)
+{
+    return a.r[0] * b.r[0] + a.r[1] * b.r[1] + a.r[2] * b.r[2];
+}
+
+// Structure::calculateInverseBox (libnnp/Structure.cpp:519-546).
+void inverseBox(double const box[3][3], double inv[3][3])
+{
+    double invdet = box[0][0] * box[1][1] * box[2][2]
+                  + box[1][0] * box[2][1] * box[0][2]
+                  + box[2][0] * box[0][1] * box[1][2]
+                  - box[2][0] * box[1][1] * box[0][2]
+                  - box[0][0] * box[2][1] * box[1][2]
+                  - box[1][0] * box[0][1] * box[2][2];
+    invdet = 1.0 / invdet;
+    inv[0][0] = box[1][1] * box[2][2] - box[2][1] * box[1][2];
+    inv[0][1] = box[2][1] * box[0][2] - box[0][1] * box[2][2];
+    inv[0][2] = box[0][1] * box[1][2] - box[1][1] * box[0][2];
+    inv[1][0] = box[2][0] * box[1][2] - box[1][0] * box[2][2];
+    inv[1][1] = box[0][0] * box[2][2] - box[2][0] * box[0][2];
+    inv[1][2] = box[1][0] * box[0][2] - box[0][0] * box[1][2];
+    inv[2][0] = box[1][0] * box[2][1] - box[2][0] * box[1][1];
+    inv[2][1] = box[2][0] * box[0][1] - box[0][0] * box[2][1];
+    inv[2][2] = box[0][0] * box[1][1] - box[1][0] * box[0][1];
+    for (int k = 0; k < 3; ++k)
+        for (int c = 0; c < 3; ++c) inv[k][c] *= invdet;
+}
+
+// Structure::calculatePbcCopies (libnnp/Structure.cpp:486-517); also returns
+// the perpendicular widths used for the cell grid.
+void pbcCopies(double const box[3][3], double rc, int pbc[3], double proj[3])
+{
+    V3 a{{box[0][0], box[0][1], box[0][2]}};
+    V3 b{{box[1][0], box[1][1], box[1][2]}};
+    V3 c{{box[2][0], box[2][1], box[2][2]}};
+    V3 const axb = normalized(cross(a, b));
+    V3 const axc = normalized(cross(a, c));
+    V3 const bxc = normalized(cross(b, c));
+    proj[0] = std::fabs(dot(a, bxc));
+    proj[1] = std::fabs(dot(b, axc));
+    proj[2] = std::fabs(dot(c, axb));
+    for (int k = 0; k < 3; ++k)
+    {
+        pbc[k] = 0;
+        while (pbc[k] * proj[k] <= rc) pbc[k]++;
+    }
+}
+
+__global__ void statusResetKernel(int* status)
+{
+    if (threadIdx.x < ST_NUM) status[threadIdx.x] = 0;
+    if (threadIdx.x == ST_BAD_ATOM) status[threadIdx.x] = -1;
+}
+
+} // namespace
+
+struct n2p2b_context
+{
+    int          device = 0;
+    cudaStream_t stream = nullptr;
+    bool         ownStream = false;
+    std::string  error;
+
+    // Potential and its device tables.
+    Potential    pot;
+    bool         generic = false;
+    bool         scaled = false;
+    bool         weighted = false;
+    bool         tablesReady = false;
+    SFParams     sfp{};
+    NNParams     nnp{};
+    int          maxSF = 0;
+    int          maxSlots = 0;
+    DevBuf       sfScale, nnW, slotSF;
+
+    // Structure.
+    long         n = 0;
+    bool         periodic = false;
+    bool         remap = false;
+    double       boxPhys[3][3] = {};
+    std::vector<int32_t> elemHost;
+    NLParams     nlp{};
+    PhysBox      pb{};
+    ElemStarts   es{};
+    int          numCells = 0;
+    DevBuf       posIn, pos, elem, atomsByElem;
+    DevBuf       cellOf, cellCount, cellFill, cellStart, cellAtoms, cellStatus;
+    DevBuf       nbrCount, nbrCountElem, nbrOff;
+    long         capacity = 0;
+    DevBuf       keyTmp, key, nbrIdx, nbrEl, dx, dy, dz, dd, entryAtom, mirror;
+    DevBuf       pairF, dGdr;
+    DevBuf       G, dEdG, dGdrSelf, Ei, selfF, F, energyOut, status;
+    int*         statusHost = nullptr;
+    double*      energyHost = nullptr;
+    int          sfCap = 256;
+    int          sfGrid = 0;
+    int          sfGridCap = 0;
+    int          smCount = 0;
+
+    // Pipeline state (what the last calls computed).
+    bool haveNL = false, haveSF = false, haveSFDeriv = false, haveNN = false;
+    bool haveNNDeriv = false, haveE = false, haveF = false;
+
+    ~n2p2b_context()
+    {
+        for (DevBuf* b : {&sfScale, &nnW, &slotSF, &posIn, &pos, &elem,
+                          &atomsByElem, &cellOf, &cellCount, &cellFill,
+                          &cellStart, &cellAtoms, &cellStatus, &nbrCount,
+                          &nbrCountElem, &nbrOff, &keyTmp, &key, &nbrIdx,
+                          &nbrEl, &dx, &dy, &dz, &dd, &entryAtom, &mirror,
+                          &pairF, &dGdr, &G, &dEdG, &dGdrSelf, &Ei, &selfF,
+                          &F, &energyOut, &status})
+            b->release();
+        if (statusHost) cudaFreeHost(statusHost);
+        if (energyHost) cudaFreeHost(energyHost);
+        if (ownStream && stream) cudaStreamDestroy(stream);
+    }
+
+    void activate() { ck(cudaSetDevice(device), "cudaSetDevice"); }
+
+    // ---- potential tables ------------------------------------------------
+
+    void buildTables()
+    {
+        int const ne = pot.numElements();
+        if (ne > kMaxElem)
+            throw std::runtime_error("ERROR: More elements than the device "
+                                     "tables hold.\n");
+        maxSF = pot.maxSymmetryFunctions();
+        maxSlots = pot.maxSlots();
+        if (maxSF > kMaxSF)
+            throw std::runtime_error("ERROR: Too many symmetry functions per "
+                                     "element for the device tables.\n");
+        std::memset(&sfp, 0, sizeof(sfp));
+        sfp.numElements = ne;
+        sfp.cutoffType = pot.cutoffType;
+        sfp.maxSlots = maxSlots;
+        sfp.maxSF = maxSF;
+        sfp.PI = 4.0 * std::atan(1.0);
+        sfp.PI_2 = 2.0 * std::atan(1.0);
+        sfp.E = std::exp(1.0);
+        sfp.TANH_PRE = std::pow((sfp.E + 1 / sfp.E) / (sfp.E - 1 / sfp.E), 3);
+        std::vector<SFScale> scale((std::size_t)ne * maxSF, SFScale{0, 1, 0, 1});
+        std::vector<int16_t> slotTab((std::size_t)kMaxElem * kMaxElem
+                                     * std::max(maxSlots, 1), (int16_t)-1);
+        int gi = 0, mi = 0;
+        for (int e = 0; e < ne; ++e)
+        {
+            Element const& el = pot.elements[e];
+            sfp.groupBeg[e] = gi;
+            sfp.numSF[e] = (int)el.sfs.size();
+            for (int f = 0; f < ne; ++f)
+            {
+                sfp.numSlots[e][f] = (int)el.sfTable[f].size();
+                for (std::size_t s = 0; s < el.sfTable[f].size(); ++s)
+                {
+                    slotTab[((std::size_t)e * kMaxElem + f) * maxSlots + s] =
+                        (int16_t)el.sfTable[f][s];
+                }
+            }
+            for (auto const& g : el.groups)
+            {
+                if (gi >= kMaxGroups || mi + (int)g.members.size()
+                                        > kMaxMembers)
+                    throw std::runtime_error("ERROR: Too many symmetry "
+                                             "function groups/members for "
+                                             "the device tables.\n");
+                DevGroup& d = sfp.groups[gi++];
+                d.type = g.type;
+                d.e1 = g.e1;
+                d.e2 = g.e2;
+                d.mbeg = mi;
+                d.mcnt = (int)g.members.size();
+                d.rc = g.rc;
+                d.rc2 = g.rc * g.rc;
+                // CutoffFunction::setCutoffRadius / setCutoffParameter.
+                d.rcinv = 1.0 / g.rc;
+                d.rci = g.rc * g.cutoffAlpha;
+                d.iw = 1.0 / (g.rc - d.rci);
+                for (std::size_t k = 0; k < g.members.size(); ++k)
+                {
+                    SymFnc const& s = el.sfs[g.members[k]];
+                    DevMember& m = sfp.members[mi++];
+                    std::memset(&m, 0, sizeof(m));
+                    m.eta = s.eta;
+                    m.rs = s.rs;
+                    m.lambda = s.lambda;
+                    m.zeta = s.zeta;
+                    m.zetaInt = (int16_t)s.zetaInt;
+                    m.useIntPow = s.useIntegerPow ? 1 : 0;
+                    m.rsPositive = s.rs > 0.0 ? 1 : 0;
+                    m.sf = (int16_t)s.index;
+                    for (int f = 0; f < kMaxElem; ++f)
+                        m.slot[f] = (f < ne) ? (int16_t)s.indexPerElement[f]
+                                             : (int16_t)-1;
+                    SFScale& q = scale[(std::size_t)e * maxSF + s.index];
+                    if (g.type == 2)
+                    {
+                        m.factorNorm = s.scalingFactor;
+                        m.calcExp = 1;
+                        q.q = 1.0;
+                    }
+                    else
+                    {
+                        // SymGrpExpAngn::sortMembers + setScalingFactors.
+                        double const fn = std::pow(2.0, 1.0 - s.zeta);
+                        m.factorNorm = fn * s.scalingFactor;
+                        m.factorDeriv = 2.0 * s.eta / s.zeta / s.lambda;
+                        m.zetaLambda = s.zeta * s.lambda;
+                        SymFnc const* prev = k > 0
+                            ? &el.sfs[g.members[k - 1]] : nullptr;
+                        m.calcExp = (prev == nullptr || prev->eta != s.eta
+                                     || prev->rs != s.rs) ? 1 : 0;
+                        q.q = m.factorNorm / s.scalingFactor;
+                    }
+                    switch (s.scalingType)
+                    {
+                    case ST_NONE:        q.smin = 0.0; q.b = 1.0; q.shift = 0.0;
+                                         break;
+                    case ST_CENTER:      q.smin = 0.0; q.b = 1.0;
+                                         q.shift = s.Gmean; break;
+                    case ST_SCALE:       q.smin = s.Smin; q.b = s.scalingFactor;
+                                         q.shift = s.Gmin; break;
+                    default:             q.smin = s.Smin; q.b = s.scalingFactor;
+                                         q.shift = s.Gmean; break;
+                    }
+                }
+            }
+        }
+        sfp.groupBeg[ne] = gi;
+
+        // NN blob.
+        std::memset(&nnp, 0, sizeof(nnp));
+        nnp.numElements = ne;
+        std::vector<double> blob;
+        int maxW = 1;
+        for (int e = 0; e < ne; ++e)
+        {
+            NeuralNet const& nn = pot.elements[e].nn;
+            if (nn.numLayers > kMaxLayers)
+                throw std::runtime_error("ERROR: Too many NN layers.\n");
+            nnp.numLayers[e] = nn.numLayers;
+            nnp.normalizeNeurons = nn.normalizeNeurons ? 1 : 0;
+            for (int l = 0; l < nn.numLayers; ++l)
+            {
+                nnp.width[e][l] = nn.neurons[l];
+                nnp.act[e][l] = nn.activations[l];
+                maxW = std::max(maxW, nn.neurons[l]);
+            }
+            for (int l = 1; l < nn.numLayers; ++l)
+            {
+                int const ni = nn.neurons[l - 1], no = nn.neurons[l];
+                nnp.woff[e][l] = (long)blob.size();
+                blob.insert(blob.end(), nn.W[l].begin(), nn.W[l].end());
+                nnp.wtoff[e][l] = (long)blob.size();
+                for (int j = 0; j < ni; ++j)
+                    for (int o = 0; o < no; ++o)
+                        blob.push_back(nn.W[l][(std::size_t)o * ni + j]);
+                nnp.boff[e][l] = (long)blob.size();
+                blob.insert(blob.end(), nn.b[l].begin(), nn.b[l].end());
+            }
+        }
+        if (maxW > kMaxWidth)
+            throw std::runtime_error("ERROR: NN layer wider than supported.\n");
+        nnp.maxWidth = maxW;
+
+        activate();
+        sfScale.ensure(sizeof(SFScale) * scale.size());
+        ck(cudaMemcpy(sfScale.p, scale.data(), sizeof(SFScale) * scale.size(),
+                      cudaMemcpyHostToDevice), "copy SF scaling");
+        nnW.ensure(sizeof(double) * blob.size());
+        ck(cudaMemcpy(nnW.p, blob.data(), sizeof(double) * blob.size(),
+                      cudaMemcpyHostToDevice), "copy NN weights");
+        slotSF.ensure(sizeof(int16_t) * slotTab.size());
+        ck(cudaMemcpy(slotSF.p, slotTab.data(), sizeof(int16_t) * slotTab.size(),
+                      cudaMemcpyHostToDevice), "copy slot table");
+        tablesReady = true;
+        invalidate();
+    }
+
+    void requireReady() const
+    {
+        if (!generic || !scaled || !weighted || !tablesReady)
+            throw StateError("ERROR: Potential is not set up (settings, "
+                             "scaling and weights are required).\n");
+    }
+
+    void requireStructure() const
+    {
+        if (n <= 0) throw StateError("ERROR: No structure set.\n");
+    }
+
+    void invalidate()
+    {
+        haveNL = haveSF = haveSFDeriv = haveNN = haveNNDeriv = false;
+        haveE = haveF = false;
+    }
+
+    // ---- structure -------------------------------------------------------
+
+    void setStructure(long num, double const* box, double const* posArg,
+                      int loc, int32_t const* elems, int flags)
+    {
+        requireReady();
+        if (num <= 0 || posArg == nullptr || elems == nullptr)
+            throw std::invalid_argument("ERROR: Invalid structure "
+                                        "arguments.\n");
+        if (num > 0x7ffffffeL / 2)
+            throw std::invalid_argument("ERROR: Too many atoms.\n");
+        int const ne = pot.numElements();
+        for (long i = 0; i < num; ++i)
+        {
+            if (elems[i] < 0 || elems[i] >= ne)
+                throw std::invalid_argument("ERROR: Element index out of "
+                                            "range.\n");
+        }
+        activate();
+        n = num;
+        elemHost.assign(elems, elems + num);
+        periodic = box != nullptr;
+        remap = periodic && (flags & N2P2B_REMAP);
+        double const L = pot.normalize ? pot.convLength : 1.0;
+        std::memset(&nlp, 0, sizeof(nlp));
+        std::memset(&pb, 0, sizeof(pb));
+        double const rc = pot.maxCutoffRadius;
+        nlp.rc2 = rc * rc;
+        if (periodic)
+        {
+            for (int k = 0; k < 3; ++k)
+                for (int c = 0; c < 3; ++c) boxPhys[k][c] = box[3 * k + c];
+            std::memcpy(pb.box, boxPhys, sizeof(boxPhys));
+            inverseBox(pb.box, pb.invbox);
+            nlp.periodic = 1;
+            // Structure::toNormalizedUnits: box *= convLength,
+            // invbox /= convLength.
+            for (int k = 0; k < 3; ++k)
+            {
+                for (int c = 0; c < 3; ++c)
+                {
+                    nlp.box[k][c] = pot.normalize ? pb.box[k][c] * L
+                                                  : pb.box[k][c];
+                    nlp.invbox[k][c] = pot.normalize ? pb.invbox[k][c] / L
+                                                     : pb.invbox[k][c];
+                }
+            }
+            double proj[3];
+            pbcCopies(nlp.box, rc, nlp.pbc, proj);
+            nlp.nimg = (2 * nlp.pbc[0] + 1) * (2 * nlp.pbc[1] + 1)
+                     * (2 * nlp.pbc[2] + 1);
+            bool cellOk = true;
+            long cells = 1;
+            for (int k = 0; k < 3; ++k)
+            {
+                int nc = (int)std::floor(proj[k] / (rc * (1.0 + 1e-9)));
+                nc = std::min(nc, 160);
+                if (nc < 1 || nlp.pbc[k] != 1) cellOk = false;
+                nlp.ncell[k] = nc;
+                cells *= std::max(nc, 1);
+            }
+            if (!cellOk)
+            {
+                nlp.ncell[0] = nlp.ncell[1] = nlp.ncell[2] = 0;
+                numCells = 0;
+            }
+            else numCells = (int)cells;
+        }
+        else
+        {
+            nlp.periodic = 0;
+            nlp.nimg = 1;
+            numCells = 0;
+        }
+        if ((long double)n * nlp.nimg * kMaxElem > 1.8e19L)
+            throw std::invalid_argument("ERROR: Structure too large for the "
+                                        "neighbor keys.\n");
+        // Element-sorted atom lists (brute-force enumeration order).
+        std::vector<int> byElem;
+        byElem.reserve(n);
+        std::memset(&es, 0, sizeof(es));
+        for (int e = 0; e < ne; ++e)
+        {
+            es.start[e] = (int)byElem.size();
+            for (long i = 0; i < n; ++i)
+                if (elemHost[i] == e) byElem.push_back((int)i);
+        }
+        es.start[ne] = (int)byElem.size();
+        for (int e = ne + 1; e <= kMaxElem; ++e) es.start[e] = es.start[ne];
+
+        posIn.ensure(sizeof(double) * 3 * n);
+        pos.ensure(sizeof(double) * 3 * n);
+        elem.ensure(sizeof(int) * n);
+        atomsByElem.ensure(sizeof(int) * n);
+        ck(cudaMemcpyAsync(elem.p, elemHost.data(), sizeof(int) * n,
+                           cudaMemcpyHostToDevice, stream), "copy elements");
+        ck(cudaMemcpyAsync(atomsByElem.p, byElem.data(), sizeof(int) * n,
+                           cudaMemcpyHostToDevice, stream), "copy atom lists");
+        setPositions(posArg, loc);
+        ck(cudaStreamSynchronize(stream), "structure upload");
+    }
+
+    void setPositions(double const* posArg, int loc)
+    {
+        requireStructure();
+        ck(cudaMemcpyAsync(posIn.p, posArg, sizeof(double) * 3 * n,
+                           loc == N2P2B_DEVICE ? cudaMemcpyDeviceToDevice
+                                               : cudaMemcpyHostToDevice,
+                           stream), "copy positions");
+        invalidate();
+    }
+
+    // ---- buffers ---------------------------------------------------------
+
+    void ensureStructureBuffers()
+    {
+        int const ne = pot.numElements();
+        cellOf.ensure(sizeof(int) * n);
+        cellAtoms.ensure(sizeof(int) * n);
+        cellCount.ensure(sizeof(int) * (numCells + 1));
+        cellFill.ensure(sizeof(int) * (numCells + 1));
+        cellStart.ensure(sizeof(int) * (numCells + 1));
+        cellStatus.ensure(sizeof(int) * ST_NUM);
+        nbrCount.ensure(sizeof(int) * n);
+        nbrCountElem.ensure(sizeof(int) * n * ne);
+        nbrOff.ensure(sizeof(int) * (n + 1));
+        G.ensure(sizeof(double) * n * maxSF);
+        dEdG.ensure(sizeof(double) * n * maxSF);
+        dGdrSelf.ensure(sizeof(double) * n * maxSF * 3);
+        Ei.ensure(sizeof(double) * n);
+        selfF.ensure(sizeof(double) * n * 3);
+        F.ensure(sizeof(double) * n * 3);
+        energyOut.ensure(sizeof(double) * 2);
+        status.ensure(sizeof(int) * ST_NUM);
+        if (!statusHost)
+            ck(cudaMallocHost((void**)&statusHost, sizeof(int) * ST_NUM),
+               "cudaMallocHost");
+        if (!energyHost)
+            ck(cudaMallocHost((void**)&energyHost, sizeof(double) * 2),
+               "cudaMallocHost");
+    }
+
+    void ensureEntryBuffers()
+    {
+        long const c = std::max(capacity, 1L);
+        keyTmp.ensure(sizeof(unsigned long long) * c);
+        key.ensure(sizeof(unsigned long long) * c);
+        nbrIdx.ensure(sizeof(int) * c);
+        nbrEl.ensure(sizeof(int8_t) * c);
+        dx.ensure(sizeof(double) * c);
+        dy.ensure(sizeof(double) * c);
+        dz.ensure(sizeof(double) * c);
+        dd.ensure(sizeof(double) * c);
+        entryAtom.ensure(sizeof(int) * c);
+        mirror.ensure(sizeof(int) * c);
+        pairF.ensure(sizeof(double) * 3 * c);
+        dGdr.ensure(sizeof(double) * 3 * (std::size_t)c
+                    * std::max(maxSlots, 1));
+    }
+
+    void grow(long total)
+    {
+        capacity = std::max(capacity, (long)(total * 1.15) + 1024);
+        ensureEntryBuffers();
+    }
+
+    // ---- pipeline stages (enqueue only) -----------------------------------
+
+    void enqueueReset()
+    {
+        statusResetKernel<<<1, 32, 0, stream>>>(status.as<int>());
+        statusResetKernel<<<1, 32, 0, stream>>>(cellStatus.as<int>());
+    }
+
+    void enqueueNL()
+    {
+        NLLaunch L;
+        L.n = (int)n;
+        L.numElements = pot.numElements();
+        L.numCells = numCells;
+        L.capacity = capacity;
+        L.p = nlp;
+        L.pb = pb;
+        L.doRemap = remap ? 1 : 0;
+        L.normalize = pot.normalize ? 1 : 0;
+        L.convLength = pot.convLength;
+        L.posIn = posIn.as<double>();
+        L.pos = pos.as<double>();
+        L.elem = elem.as<int>();
+        L.atomsByElem = atomsByElem.as<int>();
+        L.es = es;
+        L.cellOf = cellOf.as<int>();
+        L.cellCount = cellCount.as<int>();
+        L.cellStart = cellStart.as<int>();
+        L.cellFill = cellFill.as<int>();
+        L.cellAtoms = cellAtoms.as<int>();
+        L.cellScanStatus = cellStatus.as<int>();
+        L.nbrCount = nbrCount.as<int>();
+        L.nbrCountElem = nbrCountElem.as<int>();
+        L.nbrOff = nbrOff.as<int>();
+        L.keyTmp = keyTmp.as<unsigned long long>();
+        L.key = key.as<unsigned long long>();
+        L.nbrIdx = nbrIdx.as<int>();
+        L.nbrEl = nbrEl.as<int8_t>();
+        L.dx = dx.as<double>();
+        L.dy = dy.as<double>();
+        L.dz = dz.as<double>();
+        L.dd = dd.as<double>();
+        L.entryAtom = entryAtom.as<int>();
+        L.mirror = mirror.as<int>();
+        L.status = status.as<int>();
+        launchNeighborList(L, stream);
+    }
+
+    void enqueueSF(bool deriv)
+    {
+        if (sfGrid == 0 || sfGridCap != sfCap)
+        {
+            ck(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount,
+                                      device), "device attribute");
+            sfGrid = smCount * sfBlocksPerSM(sfp, sfCap);
+            sfGridCap = sfCap;
+        }
+        SFLaunch L;
+        L.n = (int)n;
+        L.derivatives = deriv ? 1 : 0;
+        L.cap = sfCap;
+        L.memberChunk = 12;
+        L.grid = (int)std::min<long>(sfGrid, n);
+        L.elem = elem.as<int>();
+        L.nbrOff = nbrOff.as<int>();
+        L.nbrCountElem = nbrCountElem.as<int>();
+        L.dx = dx.as<double>();
+        L.dy = dy.as<double>();
+        L.dz = dz.as<double>();
+        L.dd = dd.as<double>();
+        L.scale = sfScale.as<SFScale>();
+        L.G = G.as<double>();
+        L.dGdrSelf = dGdrSelf.as<double>();
+        L.dGdr = dGdr.as<double>();
+        L.status = status.as<int>();
+        launchSymmetryFunctions(sfp, L, stream);
+    }
+
+    void enqueueNN(bool deriv)
+    {
+        NNLaunch L;
+        L.n = (int)n;
+        L.derivatives = deriv ? 1 : 0;
+        L.maxSF = maxSF;
+        L.elem = elem.as<int>();
+        L.weights = nnW.as<double>();
+        L.G = G.as<double>();
+        L.energy = Ei.as<double>();
+        L.dEdG = dEdG.as<double>();
+        L.status = status.as<int>();
+        launchNeuralNetworks(nnp, L, stream);
+    }
+
+    void enqueueEnergy()
+    {
+        EnergyLaunch L;
+        L.n = (int)n;
+        L.atomicEnergy = Ei.as<double>();
+        L.out = energyOut.as<double>();
+        L.convEnergy = pot.convEnergy;
+        L.meanEnergy = pot.meanEnergy;
+        L.normalize = pot.normalize ? 1 : 0;
+        int const ne = pot.numElements();
+        L.numElements = ne;
+        for (int e = 0; e < ne; ++e)
+        {
+            long cnt = es.start[e + 1] - es.start[e];
+            L.offsetTerm[e] = cnt * pot.elements[e].atomicEnergyOffset;
+        }
+        L.status = status.as<int>();
+        launchEnergy(L, stream);
+    }
+
+    void enqueueForces()
+    {
+        ForceLaunch L;
+        int const ne = pot.numElements();
+        L.n = (int)n;
+        L.numElements = ne;
+        L.maxSF = maxSF;
+        L.maxSlots = maxSlots;
+        L.elem = elem.as<int>();
+        L.nbrOff = nbrOff.as<int>();
+        L.nbrIdx = nbrIdx.as<int>();
+        L.nbrEl = nbrEl.as<int8_t>();
+        L.mirror = mirror.as<int>();
+        L.slotSF = slotSF.as<int16_t>();
+        for (int e = 0; e < ne; ++e)
+        {
+            L.numSF[e] = sfp.numSF[e];
+            for (int f = 0; f < ne; ++f) L.numSlots[e][f] = sfp.numSlots[e][f];
+        }
+        L.dEdG = dEdG.as<double>();
+        L.dGdrSelf = dGdrSelf.as<double>();
+        L.dGdr = dGdr.as<double>();
+        L.selfF = selfF.as<double>();
+        L.pairF = pairF.as<double>();
+        L.F = F.as<double>();
+        L.forceScale = pot.normalize ? pot.convEnergy / pot.convLength : 1.0;
+        L.status = status.as<int>();
+        launchForces(L, stream);
+    }
+
+    void checkLaunch(char const* what)
+    {
+        ck(cudaGetLastError(), what);
+    }
+
+    // Reads the status words (synchronizes the stream).
+    int readStatus()
+    {
+        ck(cudaMemcpyAsync(statusHost, status.p, sizeof(int) * ST_NUM,
+                           cudaMemcpyDeviceToHost, stream), "read status");
+        ck(cudaStreamSynchronize(stream), "synchronize");
+        return statusHost[ST_FLAGS];
+    }
+
+    // Runs `stages` (bit 0 NL, 1 SF, 2 NN, 3 E, 4 F) with capacity retries.
+    void run(int stages, bool sfDeriv, bool nnDeriv)
+    {
+        requireReady();
+        requireStructure();
+        activate();
+        ensureStructureBuffers();
+        ensureEntryBuffers();
+        for (int attempt = 0; attempt < 6; ++attempt)
+        {
+            enqueueReset();
+            int st = stages;
+            // Later stages need the neighbor list of this run.
+            if (st & 1) enqueueNL();
+            if (st & 2) enqueueSF(sfDeriv);
+            if (st & 4) enqueueNN(nnDeriv);
+            if (st & 8) enqueueEnergy();
+            if (st & 16) enqueueForces();
+            checkLaunch("kernel launch");
+            int const flags = readStatus();
+            if (flags & FLAG_NBR_OVERFLOW)
+            {
+                grow(statusHost[ST_TOTAL_NBR]);
+                stages |= 1;
+                continue;
+            }
+            if (flags & FLAG_SF_CAPACITY)
+            {
+                int const need = statusHost[ST_MAX_NBR] > 0
+                               ? statusHost[ST_MAX_NBR] : sfCap * 2;
+                int const cap = ((need + 31) / 32) * 32;
+                std::size_t const shm = sfSharedBytes(sfp, cap);
+                if (shm > 227 * 1024)
+                    throw CapacityError("ERROR: An atom has more neighbors "
+                                        "than the symmetry-function kernel "
+                                        "can stage.\n");
+                sfCap = std::max(cap, sfCap + 32);
+                continue;
+            }
+            if (flags & FLAG_MIRROR_MISSING)
+                throw std::runtime_error("ERROR: Internal: neighbor list is "
+                                         "not symmetric.\n");
+            if (stages & 1) haveNL = true;
+            if (stages & 2) { haveSF = true; haveSFDeriv = sfDeriv; }
+            if (stages & 4) { haveNN = true; haveNNDeriv = nnDeriv; }
+            if (stages & 8) haveE = true;
+            if (stages & 16) haveF = true;
+            return;
+        }
+        throw CapacityError("ERROR: Capacity retries exhausted.\n");
+    }
+
+    // Full evaluation enqueued without synchronization (capacities known).
+    void enqueueAll(bool forces)
+    {
+        requireReady();
+        requireStructure();
+        if (capacity <= 0)
+            throw StateError("ERROR: evaluate_async needs known capacities: "
+                             "run n2p2b_evaluate once first.\n");
+        enqueueReset();
+        enqueueNL();
+        enqueueSF(forces);
+        enqueueNN(forces);
+        enqueueEnergy();
+        if (forces) enqueueForces();
+        checkLaunch("kernel launch");
+    }
+
+    int finishStatus()
+    {
+        int const flags = readStatus();
+        if (flags & (FLAG_NBR_OVERFLOW | FLAG_SF_CAPACITY))
+            throw CapacityError("ERROR: Capacity exceeded during an "
+                                "asynchronous evaluation; call "
+                                "n2p2b_evaluate to grow the buffers.\n");
+        if (flags & FLAG_MIRROR_MISSING)
+            throw std::runtime_error("ERROR: Internal: neighbor list is not "
+                                     "symmetric.\n");
+        haveNL = haveSF = haveNN = haveE = true;
+        return 0;
+    }
+
+    long totalEntries()
+    {
+        int off = 0;
+        ck(cudaMemcpy(&off, nbrOff.as<int>() + n, sizeof(int),
+                      cudaMemcpyDeviceToHost), "read offsets");
+        return off;
+    }
+
+    // Host permutation from device (element-grouped) order to the
+    // reference's list order (j ascending, then image).
+    void refOrder(std::vector<int>& off, std::vector<long>& perm)
+    {
+        long const E = totalEntries();
+        off.resize(n + 1);
+        ck(cudaMemcpy(off.data(), nbrOff.p, sizeof(int) * (n + 1),
+                      cudaMemcpyDeviceToHost), "read offsets");
+        std::vector<unsigned long long> k(E);
+        if (E > 0)
+            ck(cudaMemcpy(k.data(), key.p, sizeof(unsigned long long) * E,
+                          cudaMemcpyDeviceToHost), "read keys");
+        unsigned long long const mod = (unsigned long long)n * nlp.nimg;
+        perm.resize(E);
+        for (long i = 0; i < n; ++i)
+        {
+            long const b = off[i], e = off[i + 1];
+            std::iota(perm.begin() + b, perm.begin() + e, b);
+            std::sort(perm.begin() + b, perm.begin() + e,
+                      [&](long x, long y) { return k[x] % mod < k[y] % mod; });
+        }
+    }
+};
+
+// ---- C-ABI -----------------------------------------------------------------
+
+namespace
+{
+
+template <typename F>
+int guarded(n2p2b_context* ctx, F&& f)
+{
+    if (ctx == nullptr) return N2P2B_ERR_ARGUMENT;
+    try
+    {
+        f();
+        ctx->error.clear();
+        return N2P2B_OK;
+    }
+    catch (CudaError const& e)
+    {
+        ctx->error = e.what();
+        return N2P2B_ERR_CUDA;
+    }
+    catch (CapacityError const& e)
+    {
+        ctx->error = e.what();
+        return N2P2B_ERR_CAPACITY;
+    }
+    catch (StateError const& e)
+    {
+        ctx->error = e.what();
+        return N2P2B_ERR_STATE;
+    }
+    catch (std::invalid_argument const& e)
+    {
+        ctx->error = e.what();
+        return N2P2B_ERR_ARGUMENT;
+    }
+    catch (std::exception const& e)
+    {
+        ctx->error = e.what();
+        return N2P2B_ERR_SETUP;
+    }
+}
+
+} // namespace
+
+extern "C"
+{
+
+int n2p2b_create(int device, n2p2b_context** out)
+{
+    if (out == nullptr) return N2P2B_ERR_ARGUMENT;
+    *out = nullptr;
+    int count = 0;
+    if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0
+        || device >= count)
+        return N2P2B_ERR_CUDA;
+    n2p2b_context* c = new n2p2b_context();
+    c->device = device;
+    if (cudaSetDevice(device) != cudaSuccess
+        || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking)
+           != cudaSuccess)
+    {
+        delete c;
+        return N2P2B_ERR_CUDA;
+    }
+    c->ownStream = true;
+    *out = c;
+    return N2P2B_OK;
+}
+
+void n2p2b_destroy(n2p2b_context* ctx)
+{
+    if (ctx == nullptr) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    delete ctx;
+}
+
+char const* n2p2b_last_error(n2p2b_context const* ctx)
+{
+    return ctx ? ctx->error.c_str() : "null context";
+}
+
+int n2p2b_set_stream(n2p2b_context* ctx, void* stream)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        if (ctx->ownStream && ctx->stream)
+        {
+            cudaStreamSynchronize(ctx->stream);
+            cudaStreamDestroy(ctx->stream);
+        }
+        if (stream)
+        {
+            ctx->stream = static_cast<cudaStream_t>(stream);
+            ctx->ownStream = false;
+        }
+        else
+        {
+            ck(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking),
+               "cudaStreamCreate");
+            ctx->ownStream = true;
+        }
+    });
+}
+
+int n2p2b_load_settings_file(n2p2b_context* ctx, char const* path)
+{
+    return guarded(ctx, [&] {
+        if (path == nullptr) throw std::invalid_argument("ERROR: null path");
+        ctx->pot = Potential();
+        ctx->generic = ctx->scaled = ctx->weighted = false;
+        ctx->tablesReady = false;
+        ctx->pot.loadSettingsFile(path);
+    });
+}
+
+int n2p2b_setup_generic(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] {
+        ctx->pot.setupGeneric();
+        ctx->generic = true;
+    });
+}
+
+int n2p2b_setup_symmetry_function_scaling(n2p2b_context* ctx,
+                                          char const* path)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->generic) throw StateError("ERROR: setupGeneric first.\n");
+        if (path) ctx->pot.setupSymmetryFunctionScaling(path);
+        else      ctx->pot.setupSymmetryFunctionScalingNone();
+        ctx->scaled = true;
+        if (ctx->weighted) ctx->buildTables();
+    });
+}
+
+int n2p2b_setup_neural_network_weights(n2p2b_context* ctx, char const* format)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->generic) throw StateError("ERROR: setupGeneric first.\n");
+        if (format == nullptr) throw std::invalid_argument("ERROR: format");
+        ctx->pot.setupNeuralNetworkWeights(format);
+        ctx->weighted = true;
+        if (ctx->scaled) ctx->buildTables();
+    });
+}
+
+int n2p2b_setup(n2p2b_context* ctx, char const* directory)
+{
+    if (ctx == nullptr || directory == nullptr) return N2P2B_ERR_ARGUMENT;
+    std::string d(directory);
+    if (!d.empty() && d.back() != '/') d += "/";
+    int rc = n2p2b_load_settings_file(ctx, (d + "input.nn").c_str());
+    if (rc) return rc;
+    rc = n2p2b_setup_generic(ctx);
+    if (rc) return rc;
+    rc = n2p2b_setup_symmetry_function_scaling(ctx,
+                                               (d + "scaling.data").c_str());
+    if (rc) return rc;
+    return n2p2b_setup_neural_network_weights(
+        ctx, (d + "weights.%03zu.data").c_str());
+}
+
+int n2p2b_num_elements(n2p2b_context const* ctx)
+{
+    return ctx ? ctx->pot.numElements() : 0;
+}
+
+int n2p2b_element_symbol(n2p2b_context const* ctx, int e, char* buf,
+                         size_t len)
+{
+    if (!ctx || !buf || e < 0 || e >= ctx->pot.numElements())
+        return N2P2B_ERR_ARGUMENT;
+    std::snprintf(buf, len, "%s", ctx->pot.elements[e].symbol.c_str());
+    return N2P2B_OK;
+}
+
+int n2p2b_element_index(n2p2b_context const* ctx, char const* symbol)
+{
+    if (!ctx || !symbol) return N2P2B_ERR_ARGUMENT;
+    for (int e = 0; e < ctx->pot.numElements(); ++e)
+        if (ctx->pot.elements[e].symbol == symbol) return e;
+    return N2P2B_ERR_ARGUMENT;
+}
+
+int n2p2b_num_symmetry_functions(n2p2b_context const* ctx, int e)
+{
+    if (!ctx || e < 0 || e >= ctx->pot.numElements()) return 0;
+    return (int)ctx->pot.elements[e].sfs.size();
+}
+
+int n2p2b_num_slots(n2p2b_context const* ctx, int e, int ne)
+{
+    if (!ctx || e < 0 || ne < 0 || e >= ctx->pot.numElements()
+        || ne >= ctx->pot.numElements())
+        return 0;
+    return (int)ctx->pot.elements[e].sfTable[ne].size();
+}
+
+double n2p2b_max_cutoff_radius(n2p2b_context const* ctx)
+{
+    return ctx ? ctx->pot.maxCutoffRadius : 0.0;
+}
+
+int n2p2b_set_structure(n2p2b_context* ctx, int64_t num_atoms,
+                        double const* box, double const* positions,
+                        int positions_location, int32_t const* elements,
+                        int flags)
+{
+    return guarded(ctx, [&] {
+        ctx->setStructure((long)num_atoms, box, positions, positions_location,
+                          elements, flags);
+    });
+}
+
+int n2p2b_set_positions(n2p2b_context* ctx, double const* positions,
+                        int positions_location)
+{
+    return guarded(ctx, [&] {
+        if (!positions) throw std::invalid_argument("ERROR: positions");
+        ctx->activate();
+        ctx->setPositions(positions, positions_location);
+    });
+}
+
+int n2p2b_calculate_neighbor_list(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] { ctx->run(1, false, false); });
+}
+
+int n2p2b_calculate_symmetry_function_groups(n2p2b_context* ctx,
+                                             int derivatives)
+{
+    return guarded(ctx, [&] {
+        int st = 2;
+        if (!ctx->haveNL) st |= 1;
+        ctx->run(st, derivatives != 0, false);
+    });
+}
+
+int n2p2b_calculate_atomic_neural_networks(n2p2b_context* ctx,
+                                           int derivatives)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveSF)
+            throw StateError("ERROR: Symmetry functions not calculated.\n");
+        ctx->run(4, ctx->haveSFDeriv, derivatives != 0);
+    });
+}
+
+int n2p2b_calculate_energy(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveNN)
+            throw StateError("ERROR: Atomic NNs not calculated.\n");
+        ctx->run(8, ctx->haveSFDeriv, ctx->haveNNDeriv);
+    });
+}
+
+int n2p2b_calculate_forces(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveNN || !ctx->haveNNDeriv || !ctx->haveSFDeriv)
+            throw StateError("ERROR: Forces need symmetry-function and NN "
+                             "derivatives.\n");
+        ctx->run(16, true, true);
+    });
+}
+
+int n2p2b_evaluate(n2p2b_context* ctx, int use_forces)
+{
+    return guarded(ctx, [&] {
+        bool const f = use_forces != 0;
+        ctx->run(f ? 31 : 15, f, f);
+    });
+}
+
+int n2p2b_evaluate_async(n2p2b_context* ctx, int use_forces)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        ctx->enqueueAll(use_forces != 0);
+        ctx->haveF = use_forces != 0;
+        ctx->haveSFDeriv = ctx->haveNNDeriv = use_forces != 0;
+    });
+}
+
+int n2p2b_finish(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        ctx->finishStatus();
+    });
+}
+
+int n2p2b_get_energy(n2p2b_context* ctx, double* energy)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveE) throw StateError("ERROR: Energy not calculated.\n");
+        if (!energy) throw std::invalid_argument("ERROR: energy");
+        ctx->activate();
+        ck(cudaMemcpyAsync(ctx->energyHost, ctx->energyOut.p,
+                           sizeof(double) * 2, cudaMemcpyDeviceToHost,
+                           ctx->stream), "read energy");
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+        *energy = ctx->energyHost[1];
+    });
+}
+
+int n2p2b_get_forces(n2p2b_context* ctx, double* forces, int location)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveF) throw StateError("ERROR: Forces not calculated.\n");
+        if (!forces) throw std::invalid_argument("ERROR: forces");
+        ctx->activate();
+        ck(cudaMemcpyAsync(forces, ctx->F.p, sizeof(double) * 3 * ctx->n,
+                           location == N2P2B_DEVICE ? cudaMemcpyDeviceToDevice
+                                                    : cudaMemcpyDeviceToHost,
+                           ctx->stream), "read forces");
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+    });
+}
+
+int n2p2b_get_atomic_energies(n2p2b_context* ctx, double* energies)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveNN) throw StateError("ERROR: NNs not calculated.\n");
+        ctx->activate();
+        ck(cudaMemcpy(energies, ctx->Ei.p, sizeof(double) * ctx->n,
+                      cudaMemcpyDeviceToHost), "read atomic energies");
+        if (ctx->pot.normalize)
+            for (long i = 0; i < ctx->n; ++i)
+                energies[i] /= ctx->pot.convEnergy;
+    });
+}
+
+int n2p2b_get_neighbor_counts(n2p2b_context* ctx, int64_t* counts)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveNL) throw StateError("ERROR: No neighbor list.\n");
+        ctx->activate();
+        std::vector<int> c(ctx->n);
+        ck(cudaMemcpy(c.data(), ctx->nbrCount.p, sizeof(int) * ctx->n,
+                      cudaMemcpyDeviceToHost), "read counts");
+        for (long i = 0; i < ctx->n; ++i) counts[i] = c[i];
+    });
+}
+
+int n2p2b_get_neighbor_list(n2p2b_context* ctx, int64_t* index, double* dr,
+                            double* d)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveNL) throw StateError("ERROR: No neighbor list.\n");
+        ctx->activate();
+        std::vector<int> off;
+        std::vector<long> perm;
+        ctx->refOrder(off, perm);
+        long const E = (long)perm.size();
+        std::vector<int> idx(E);
+        std::vector<double> x(E), y(E), z(E), dd(E);
+        if (E > 0)
+        {
+            ck(cudaMemcpy(idx.data(), ctx->nbrIdx.p, sizeof(int) * E,
+                          cudaMemcpyDeviceToHost), "read");
+            ck(cudaMemcpy(x.data(), ctx->dx.p, sizeof(double) * E,
+                          cudaMemcpyDeviceToHost), "read");
+            ck(cudaMemcpy(y.data(), ctx->dy.p, sizeof(double) * E,
+                          cudaMemcpyDeviceToHost), "read");
+            ck(cudaMemcpy(z.data(), ctx->dz.p, sizeof(double) * E,
+                          cudaMemcpyDeviceToHost), "read");
+            ck(cudaMemcpy(dd.data(), ctx->dd.p, sizeof(double) * E,
+                          cudaMemcpyDeviceToHost), "read");
+        }
+        for (long e = 0; e < E; ++e)
+        {
+            long const s = perm[e];
+            if (index) index[e] = idx[s];
+            if (dr)
+            {
+                dr[3 * e + 0] = x[s];
+                dr[3 * e + 1] = y[s];
+                dr[3 * e + 2] = z[s];
+            }
+            if (d) d[e] = dd[s];
+        }
+    });
+}
+
+int n2p2b_get_symmetry_functions(n2p2b_context* ctx, double* G, int stride)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveSF) throw StateError("ERROR: No symmetry functions.\n");
+        if (stride < ctx->maxSF) throw std::invalid_argument("ERROR: stride");
+        ctx->activate();
+        std::vector<double> g((std::size_t)ctx->n * ctx->maxSF);
+        ck(cudaMemcpy(g.data(), ctx->G.p, sizeof(double) * g.size(),
+                      cudaMemcpyDeviceToHost), "read G");
+        for (long i = 0; i < ctx->n; ++i)
+        {
+            int const ns = ctx->sfp.numSF[ctx->elemHost[i]];
+            for (int s = 0; s < ns; ++s)
+                G[(std::size_t)i * stride + s] = g[(std::size_t)i * ctx->maxSF + s];
+        }
+    });
+}
+
+int n2p2b_get_dEdG(n2p2b_context* ctx, double* out, int stride)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveNN || !ctx->haveNNDeriv)
+            throw StateError("ERROR: No dE/dG.\n");
+        if (stride < ctx->maxSF) throw std::invalid_argument("ERROR: stride");
+        ctx->activate();
+        std::vector<double> g((std::size_t)ctx->n * ctx->maxSF);
+        ck(cudaMemcpy(g.data(), ctx->dEdG.p, sizeof(double) * g.size(),
+                      cudaMemcpyDeviceToHost), "read dEdG");
+        for (long i = 0; i < ctx->n; ++i)
+        {
+            int const ns = ctx->sfp.numSF[ctx->elemHost[i]];
+            for (int s = 0; s < ns; ++s)
+                out[(std::size_t)i * stride + s] =
+                    g[(std::size_t)i * ctx->maxSF + s];
+        }
+    });
+}
+
+int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sfStride,
+                   double* neighbor, int slotStride)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveSF || !ctx->haveSFDeriv)
+            throw StateError("ERROR: No symmetry-function derivatives.\n");
+        if (sfStride < ctx->maxSF || slotStride < ctx->maxSlots)
+            throw std::invalid_argument("ERROR: stride");
+        ctx->activate();
+        long const n = ctx->n;
+        int const S = ctx->maxSlots;
+        if (self)
+        {
+            std::vector<double> g((std::size_t)n * ctx->maxSF * 3);
+            ck(cudaMemcpy(g.data(), ctx->dGdrSelf.p, sizeof(double) * g.size(),
+                          cudaMemcpyDeviceToHost), "read dGdr self");
+            for (long i = 0; i < n; ++i)
+            {
+                int const ns = ctx->sfp.numSF[ctx->elemHost[i]];
+                for (int s = 0; s < ns; ++s)
+                    for (int c = 0; c < 3; ++c)
+                        self[((std::size_t)i * sfStride + s) * 3 + c] =
+                            g[((std::size_t)i * ctx->maxSF + s) * 3 + c];
+            }
+        }
+        if (neighbor)
+        {
+            std::vector<int> off;
+            std::vector<long> perm;
+            ctx->refOrder(off, perm);
+            long const E = (long)perm.size();
+            std::vector<double> g((std::size_t)E * S * 3);
+            std::vector<int8_t> el(E);
+            if (E > 0)
+            {
+                ck(cudaMemcpy(g.data(), ctx->dGdr.p, sizeof(double) * g.size(),
+                              cudaMemcpyDeviceToHost), "read dGdr");
+                ck(cudaMemcpy(el.data(), ctx->nbrEl.p, E,
+                              cudaMemcpyDeviceToHost), "read elements");
+            }
+            std::vector<long> atomOf(E);
+            for (long i = 0; i < n; ++i)
+                for (long e = off[i]; e < off[i + 1]; ++e) atomOf[e] = i;
+            for (long e = 0; e < E; ++e)
+            {
+                long const s = perm[e];
+                long const i = atomOf[s];
+                long const cnt = off[i + 1] - off[i];
+                long const t = s - off[i];
+                double const* blk = g.data() + (std::size_t)off[i] * S * 3;
+                int const ns = ctx->sfp.numSlots[ctx->elemHost[i]][el[s]];
+                for (int k = 0; k < ns; ++k)
+                    for (int c = 0; c < 3; ++c)
+                        neighbor[((std::size_t)e * slotStride + k) * 3 + c] =
+                            blk[((std::size_t)k * 3 + c) * cnt + t];
+            }
+        }
+    });
+}
+
+int n2p2b_predict(n2p2b_context* ctx, int64_t num_atoms, double const* box,
+                  double const* positions, int32_t const* elements,
+                  double* energy, double* forces)
+{
+    int rc = n2p2b_set_structure(ctx, num_atoms, box, positions, N2P2B_HOST,
+                                 elements, N2P2B_REMAP);
+    if (rc) return rc;
+    rc = n2p2b_evaluate(ctx, forces != nullptr);
+    if (rc) return rc;
+    if (energy)
+    {
+        rc = n2p2b_get_energy(ctx, energy);
+        if (rc) return rc;
+    }
+    if (forces) rc = n2p2b_get_forces(ctx, forces, N2P2B_HOST);
+    return rc;
+}
+
+} // extern "C"

@@ -1,0 +1,337 @@
+// Atomic neural networks, forces and energy (FP64 plain form).
+//
+// NN: NeuralNetwork::propagate / propagateLayer (libnnp/NeuralNetwork.cpp:
+// 386-394, 761-896) and NeuralNetwork::calculateDEdG (:396-442).  The
+// reference computes dE/dG in forward mode, one input at a time; here it is
+// the reverse-mode sweep (one backward pass of the single output), the same
+// derivative up to summation order.  One warp per atom, lanes over neurons;
+// W^T (in-major) for the forward sweep and W (out-major) for the backward
+// sweep so both read coalesced rows.
+//
+// Forces: Mode::calculateForces (libnnp/Mode.cpp:1849-1912) with
+// Atom::calculateSelfForceShort / calculatePairForceShort (libnnp/Atom.cpp:
+// 371-401).  The reference gathers, for atom i, the pair terms of every entry
+// (j -> i) in the lists of i's unique neighbors j != i.  By list symmetry
+// those entries are exactly the mirrors of i's own entries (i -> j, bc), so:
+//   pass 1 (warp per owner atom j, lanes over its entries, coalesced reads
+//           of the stored dG/dr):  pairF[e] = -sum_s dEdG_j[table(s)] dGdr[e][s]
+//           and selfF[j] = -sum_s dEdG_j[s] dGdr_self[j][s];
+//   pass 2 (thread per atom i): F_i = selfF_i + sum over i's entries e with
+//           index != i of pairF[mirror[e]]
+// -- a fixed-order segmented reduction, no atomics.  Entries of i pointing to
+// i itself (periodic self-images) are skipped exactly as the reference skips
+// i in neighborsUnique.
+#include "device_common.cuh"
+#include "kernels.h"
+
+namespace n2p2b
+{
+
+namespace
+{
+
+constexpr int kNNWarps = 4;
+constexpr double kExpLimit = 35.0;  // EXP_LIMIT, libnnp/NeuralNetwork.cpp:25
+
+// Activation value and derivative (NeuralNetwork::propagateLayer).
+__device__ __forceinline__ void activate(int a, double x, double& v,
+                                         double& dv)
+{
+    switch (a)
+    {
+    case 0: // AF_IDENTITY
+        v = x;
+        dv = 1.0;
+        return;
+    case 1: // AF_TANH
+    {
+        double const t = tanh(x);
+        v = t;
+        dv = 1.0 - t * t;
+        return;
+    }
+    case 2: // AF_LOGISTIC
+        if (x > kExpLimit) { v = 1.0; dv = 0.0; return; }
+        if (x < -kExpLimit) { v = 0.0; dv = 0.0; return; }
+        {
+            double const t = 1.0 / (1.0 + exp(-x));
+            v = t;
+            dv = t * (1.0 - t);
+        }
+        return;
+    case 3: // AF_SOFTPLUS
+        if (x > kExpLimit) { v = x; dv = 1.0; return; }
+        if (x < -kExpLimit) { v = 0.0; dv = 0.0; return; }
+        {
+            double const t = exp(x);
+            v = log(1.0 + t);
+            dv = 1.0 / (1.0 + 1.0 / t);
+        }
+        return;
+    case 4: // AF_RELU
+        if (x > 0.0) { v = x; dv = 1.0; }
+        else { v = 0.0; dv = 0.0; }
+        return;
+    case 5: // AF_GAUSSIAN
+    {
+        double const t = exp(-0.5 * x * x);
+        v = t;
+        dv = -x * t;
+        return;
+    }
+    case 6: // AF_COS
+        v = cos(x);
+        dv = -sin(x);
+        return;
+    case 7: // AF_REVLOGISTIC
+    {
+        double const t = 1.0 / (1.0 + exp(-x));
+        v = 1.0 - t;
+        dv = t * (t - 1.0);
+        return;
+    }
+    case 8: // AF_EXP
+    {
+        double const t = exp(-x);
+        v = t;
+        dv = -t;
+        return;
+    }
+    default: // AF_HARMONIC
+        v = x * x;
+        dv = 2.0 * x;
+        return;
+    }
+}
+
+// Warp per atom.  Shared memory per warp: activations of the current layer
+// (maxWidth) and the activation derivatives of every layer (L * maxWidth).
+__global__ void __launch_bounds__(32 * kNNWarps)
+nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
+{
+    extern __shared__ double smem[];
+    int const lane = threadIdx.x & 31;
+    int const w = threadIdx.x >> 5;
+    int const W = P.maxWidth;
+    double* x = smem + (long)w * W * (kMaxLayers + 2);
+    double* y = x + W;
+    double* dfs = y + W;  // [layer][W]
+    if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    for (int i = blockIdx.x * kNNWarps + w; i < L.n;
+         i += gridDim.x * kNNWarps)
+    {
+        int const e = L.elem[i];
+        int const nl = P.numLayers[e];
+        int const nin = P.width[e][0];
+        double const* g = L.G + (long)i * L.maxSF;
+        for (int k = lane; k < nin; k += 32) x[k] = g[k];
+        __syncwarp();
+        double out = 0.0;
+        for (int l = 1; l < nl; ++l)
+        {
+            int const ni = P.width[e][l - 1];
+            int const no = P.width[e][l];
+            double const* Wt = L.weights + P.wtoff[e][l];
+            double const* b = L.weights + P.boff[e][l];
+            int const act = P.act[e][l];
+            for (int o = lane; o < no; o += 32)
+            {
+                double acc = 0.0;
+                for (int j = 0; j < ni; ++j) acc += Wt[(long)j * no + o] * x[j];
+                acc += b[o];
+                if (P.normalizeNeurons) acc /= ni;
+                double v, dv;
+                activate(act, acc, v, dv);
+                y[o] = v;
+                dfs[l * W + o] = dv;
+            }
+            __syncwarp();
+            for (int o = lane; o < no; o += 32) x[o] = y[o];
+            __syncwarp();
+        }
+        out = x[0];
+        if (lane == 0) L.energy[i] = out;
+        if (L.derivatives)
+        {
+            // delta_L = f'_L (/ n_{L-1}); delta_{l-1}[j] =
+            //   f'_{l-1}[j] * sum_o W_l[o][j] delta_l[o] (/ n_{l-2})
+            int const nlast = P.width[e][nl - 2];
+            double* d = y;  // delta of the current layer
+            if (lane == 0)
+            {
+                double v = dfs[(nl - 1) * W + 0];
+                if (P.normalizeNeurons) v /= nlast;
+                d[0] = v;
+            }
+            __syncwarp();
+            for (int l = nl - 1; l >= 1; --l)
+            {
+                int const ni = P.width[e][l - 1];
+                int const no = P.width[e][l];
+                double const* Wm = L.weights + P.woff[e][l];
+                for (int j = lane; j < ni; j += 32)
+                {
+                    double acc = 0.0;
+                    for (int o = 0; o < no; ++o)
+                        acc += Wm[(long)o * ni + j] * d[o];
+                    if (l > 1)
+                    {
+                        acc *= dfs[(l - 1) * W + j];
+                        if (P.normalizeNeurons) acc /= P.width[e][l - 2];
+                    }
+                    x[j] = acc;
+                }
+                __syncwarp();
+                for (int j = lane; j < ni; j += 32) d[j] = x[j];
+                __syncwarp();
+            }
+            double* o = L.dEdG + (long)i * L.maxSF;
+            for (int k = lane; k < nin; k += 32) o[k] = d[k];
+        }
+        __syncwarp();
+    }
+}
+
+// Pass 1: warp per owner atom j.
+__global__ void __launch_bounds__(128)
+pairForceKernel(ForceLaunch const L)
+{
+    extern __shared__ double smem[];
+    int const lane = threadIdx.x & 31;
+    int const w = threadIdx.x >> 5;
+    int const warps = blockDim.x >> 5;
+    double* dE = smem + (long)w * L.maxSF;
+    if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    for (int j = blockIdx.x * warps + w; j < L.n; j += gridDim.x * warps)
+    {
+        int const ej = L.elem[j];
+        double const* src = L.dEdG + (long)j * L.maxSF;
+        for (int s = lane; s < L.maxSF; s += 32) dE[s] = src[s];
+        __syncwarp();
+        // Self force.
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        double const* gs = L.dGdrSelf + (long)j * L.maxSF * 3;
+        int const numSF = L.numSF[ej];
+        for (int s = lane; s < numSF; s += 32)
+        {
+            fx -= dE[s] * gs[s * 3 + 0];
+            fy -= dE[s] * gs[s * 3 + 1];
+            fz -= dE[s] * gs[s * 3 + 2];
+        }
+        fx = warpSum(fx);
+        fy = warpSum(fy);
+        fz = warpSum(fz);
+        if (lane == 0)
+        {
+            L.selfF[(long)j * 3 + 0] = fx;
+            L.selfF[(long)j * 3 + 1] = fy;
+            L.selfF[(long)j * 3 + 2] = fz;
+        }
+        // Pair terms of j's entries.
+        long const b = L.nbrOff[j];
+        int const cnt = L.nbrOff[j + 1] - (int)b;
+        double const* gd = L.dGdr + b * (long)L.maxSlots * 3;
+        for (int t = lane; t < cnt; t += 32)
+        {
+            int const en = L.nbrEl[b + t];
+            int const ns = L.numSlots[ej][en];
+            int16_t const* tab = L.slotSF + ((long)ej * kMaxElem + en)
+                                            * L.maxSlots;
+            double px = 0.0, py = 0.0, pz = 0.0;
+            for (int s = 0; s < ns; ++s)
+            {
+                double const c = dE[tab[s]];
+                px -= c * gd[((long)s * 3 + 0) * cnt + t];
+                py -= c * gd[((long)s * 3 + 1) * cnt + t];
+                pz -= c * gd[((long)s * 3 + 2) * cnt + t];
+            }
+            L.pairF[(b + t) * 3 + 0] = px;
+            L.pairF[(b + t) * 3 + 1] = py;
+            L.pairF[(b + t) * 3 + 2] = pz;
+        }
+        __syncwarp();
+    }
+}
+
+// Pass 2: thread per atom.
+__global__ void gatherForceKernel(ForceLaunch const L)
+{
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= L.n) return;
+    if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    double fx = L.selfF[(long)i * 3 + 0];
+    double fy = L.selfF[(long)i * 3 + 1];
+    double fz = L.selfF[(long)i * 3 + 2];
+    for (int e = L.nbrOff[i]; e < L.nbrOff[i + 1]; ++e)
+    {
+        if (L.nbrIdx[e] == i) continue;
+        long const m = L.mirror[e];
+        if (m < 0) continue;  // flagged by the mirror kernel; never read OOB
+        fx += L.pairF[m * 3 + 0];
+        fy += L.pairF[m * 3 + 1];
+        fz += L.pairF[m * 3 + 2];
+    }
+    // Atom::toPhysicalUnits: f /= convEnergy / convLength.
+    L.F[(long)i * 3 + 0] = fx / L.forceScale;
+    L.F[(long)i * 3 + 1] = fy / L.forceScale;
+    L.F[(long)i * 3 + 2] = fz / L.forceScale;
+}
+
+// Deterministic energy sum (fixed tree) + Structure::toPhysicalUnits +
+// Mode::addEnergyOffset (libnnp/Mode.cpp:2018-2035).
+__global__ void energyKernel(EnergyLaunch const L)
+{
+    __shared__ double part[1024];
+    int const t = threadIdx.x;
+    double s = 0.0;
+    for (int i = t; i < L.n; i += blockDim.x) s += L.atomicEnergy[i];
+    part[t] = s;
+    __syncthreads();
+    for (int h = blockDim.x >> 1; h > 0; h >>= 1)
+    {
+        if (t < h) part[t] += part[t + h];
+        __syncthreads();
+    }
+    if (t == 0)
+    {
+        double const en = part[0];
+        double e = en;
+        if (L.normalize)
+            e = e / L.convEnergy + (double)L.n * L.meanEnergy;
+        for (int k = 0; k < L.numElements; ++k) e += L.offsetTerm[k];
+        L.out[0] = en;
+        L.out[1] = e;
+    }
+}
+
+} // namespace
+
+void launchNeuralNetworks(NNParams const& P, NNLaunch const& L,
+                          cudaStream_t s)
+{
+    std::size_t const shm = sizeof(double) * (std::size_t)kNNWarps
+                          * P.maxWidth * (kMaxLayers + 2);
+    cudaFuncSetAttribute(nnFp64Kernel,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)shm);
+    int const grid = (L.n + kNNWarps - 1) / kNNWarps;
+    nnFp64Kernel<<<grid > 0 ? grid : 1, 32 * kNNWarps, shm, s>>>(P, L);
+}
+
+void launchForces(ForceLaunch const& L, cudaStream_t s)
+{
+    int const warps = 4;
+    std::size_t const shm = sizeof(double) * warps * (std::size_t)L.maxSF;
+    int const grid = (L.n + warps - 1) / warps;
+    pairForceKernel<<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
+    int const tb = 128;
+    gatherForceKernel<<<(L.n + tb - 1) / tb > 0 ? (L.n + tb - 1) / tb : 1, tb,
+                        0, s>>>(L);
+}
+
+void launchEnergy(EnergyLaunch const& L, cudaStream_t s)
+{
+    energyKernel<<<1, 1024, 0, s>>>(L);
+}
+
+} // namespace n2p2b

@@ -1,0 +1,98 @@
+// Plain-old-data parameter tables shared by the host builder (context.cu) and
+// the kernels.  They are passed to kernels by value as __grid_constant__
+// parameters, so every potential parameter a warp reads uniformly is served
+// from the constant bank (no load instruction, no shared-memory staging).
+#pragma once
+
+#include <cstdint>
+
+namespace n2p2b
+{
+
+constexpr int kMaxElem      = 6;    // elements per potential on the device
+constexpr int kMaxGroups    = 48;   // SF groups, all elements together
+constexpr int kMaxMembers   = 256;  // SF group members, all elements
+constexpr int kMaxSF        = 256;  // symmetry functions per element
+constexpr int kMaxLayers    = 8;    // NN layers incl. input and output
+constexpr int kMaxWidth     = 256;  // NN layer width
+
+// Symmetry-function group (SymGrpExpRad / SymGrpExpAngn / SymGrpExpAngw).
+struct DevGroup
+{
+    int    type;        // 2, 3, 9
+    int    e1, e2;      // neighbor elements (e2 == -1: radial)
+    int    mbeg, mcnt;  // member range
+    int    pad;
+    double rc, rc2;     // cutoff radius and its square
+    double rci, iw;     // CutoffFunction::rci, iw  (alpha-shifted inner cutoff)
+    double rcinv;       // 1 / rc
+};
+
+// One group member.  Angular members carry the SymGrpExpAngn::sortMembers
+// derived factors; radial members use `factorNorm` for the scaling factor.
+struct DevMember
+{
+    double  eta, rs, lambda, zeta;
+    double  factorNorm;   // angular: 2^(1-zeta) * scalingFactor; radial: sf
+    double  factorDeriv;  // 2 eta / zeta / lambda
+    double  zetaLambda;   // zeta * lambda
+    int16_t zetaInt;
+    int16_t sf;           // element-local SF index (NN input index)
+    uint8_t calcExp;      // first member of an (eta, rs) run
+    uint8_t useIntPow;
+    uint8_t rsPositive;
+    uint8_t pad;
+    int16_t slot[kMaxElem];  // dG/dr slot per neighbor element, -1 = none
+};
+
+struct SFParams
+{
+    int       numElements;
+    int       cutoffType;      // CutoffType (global in n2p2)
+    int       maxSlots;        // dG/dr slots per neighbor entry (stride)
+    int       maxSF;           // SF stride of per-atom arrays
+    int       groupBeg[kMaxElem + 1];
+    int       numSF[kMaxElem];
+    int       numSlots[kMaxElem][kMaxElem];
+    double    PI, PI_2, E, TANH_PRE;  // CutoffFunction constants, host-made
+    DevGroup  groups[kMaxGroups];
+    DevMember members[kMaxMembers];
+};
+
+// Final G transform per SF: G = Smin + b * (q * v - shift), with
+// (Smin, b, shift) chosen so that all n2p2 scaling types come out
+// exactly (SymFnc::scale): NONE -> (0, 1, 0), CENTER -> (0, 1, Gmean).
+// q = factorNorm / scalingFactor for angular SFs (SymGrpExpAngn.cpp:396),
+// 1 for radial.
+struct SFScale
+{
+    double smin, b, shift, q;
+};
+
+// Neighbor-list geometry for one structure (all values in the units the
+// kernels compute in, i.e. after normalization).
+struct NLParams
+{
+    int    periodic;
+    int    pbc[3];            // Structure::calculatePbcCopies
+    int    ncell[3];          // cells per box vector (cell path) or 0
+    int    nimg;              // (2 pbc0 + 1)(2 pbc1 + 1)(2 pbc2 + 1)
+    double box[3][3];         // box[k] = k-th box vector
+    double invbox[3][3];      // Structure::invbox rows
+    double rc2;               // (max cutoff)^2, NL test dr.norm2() <= rc2
+};
+
+struct NNParams
+{
+    int    numElements;
+    int    numLayers[kMaxElem];
+    int    width[kMaxElem][kMaxLayers];
+    int    act[kMaxElem][kMaxLayers];
+    long   woff[kMaxElem][kMaxLayers];   // offset of W (out x in) in blob
+    long   wtoff[kMaxElem][kMaxLayers];  // offset of W^T (in x out)
+    long   boff[kMaxElem][kMaxLayers];   // offset of bias
+    int    normalizeNeurons;
+    int    maxWidth;
+};
+
+} // namespace n2p2b

@@ -1,0 +1,164 @@
+"""Generates the synthetic water potentials used by the tests and the bench.
+
+    python tests/golden/make_potentials.py
+
+Writes tests/golden/potentials/<name>/{input.nn, weights.001.data,
+weights.008.data, scaling.data} for
+
+* h2o_52 -- 52 SFs per element (radial eta 0.001..1.5 per neighbor element;
+  narrow angular eta {0.001, 0.01, 0.05}, zeta {1, 4}, lambda +-1 per
+  element pair), cos cutoff rc = 12 bohr, NN 52-25-25-1 (tanh, tanh, linear);
+* h2o_92 -- the wide form: radial eta extended by {2.5, 4.0}, zeta
+  {1, 2, 4, 16}: 92 SFs, NN 92-64-64-64-1 (softplus x3, linear).
+
+Weights: seeded U[-1, 1] for every connection, then the Nguyen-Widrow
+modification of NeuralNetwork::modifyConnections(MS_NGUYENWIDROW)
+(libnnp/NeuralNetwork.cpp:269-310), restated here, in the weight order of
+NeuralNetwork::setConnections (:147-169).
+
+scaling.data: min / max / mean / sigma (n-1 normalization, the quantities
+libnnptrain/Dataset.cpp:1064-1080 writes) of the UNSCALED symmetry
+functions over 10 seeded 64-molecule water boxes, computed by the reference
+library itself (oracle/_ref, Mode::setupSymmetryFunctionScalingNone).
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from n2p2_b200 import synth  # noqa: E402
+from oracle.ref import RefModel  # noqa: E402
+
+OUT = os.path.join(HERE, "potentials")
+ELEMENTS = ["H", "O"]
+
+
+def sf_lines(radial_eta, ang_eta, zetas, rc=12.0):
+    lines = []
+    for ec in ELEMENTS:
+        for e1 in ELEMENTS:
+            for eta in radial_eta:
+                lines.append(f"symfunction_short {ec} 2 {e1} {eta} 0.0 {rc}")
+        for e1, e2 in (("H", "H"), ("H", "O"), ("O", "O")):
+            for eta in ang_eta:
+                for zeta in zetas:
+                    for lam in (-1.0, 1.0):
+                        lines.append(f"symfunction_short {ec} 3 {e1} {e2} "
+                                     f"{eta} {lam} {zeta} {rc}")
+    return lines
+
+
+def write_input_nn(d, nodes, acts, lines):
+    with open(os.path.join(d, "input.nn"), "w") as f:
+        f.write("# Synthetic water potential (generated by "
+                "tests/golden/make_potentials.py)\n")
+        f.write("number_of_elements 2\n")
+        f.write("elements H O\n")
+        f.write("cutoff_type 1 0.0\n")
+        # Centering only (ST_CENTER).  With rs = 0 and eta up to 4 bohr^-2
+        # the O-O radial functions stay between 1e-15 and 1e-39 in every
+        # generated frame (O-O >= 4.7 bohr), so min/max or sigma scaling
+        # would multiply them by up to 1e38 and make the potential
+        # numerically meaningless.
+        f.write("center_symmetry_functions\n")
+        f.write(f"global_hidden_layers_short {len(nodes)}\n")
+        f.write("global_nodes_short " + " ".join(map(str, nodes)) + "\n")
+        f.write("global_activation_short " + " ".join(acts) + "\n")
+        for ln in lines:
+            f.write(ln + "\n")
+
+
+def nguyen_widrow(layers, acts, rng):
+    """Connections (setConnections order) after U[-1,1] + Nguyen-Widrow."""
+    W = []
+    b = []
+    for i in range(1, len(layers)):
+        W.append(rng.uniform(-1.0, 1.0, size=(layers[i], layers[i - 1])))
+        b.append(rng.uniform(-1.0, 1.0, size=layers[i]))
+    for i in range(1, len(layers) - 1):
+        beta = 0.7 * math.pow(layers[i], 1.0 / float(layers[i - 1]))
+        tanh = acts[i - 1] == "t"
+        for j in range(layers[i]):
+            s = math.sqrt(float(np.sum(W[i - 1][j] ** 2)))
+            W[i - 1][j] *= beta / s
+            b[i - 1][j] *= beta
+            if tanh:
+                W[i - 1][j] *= 2.0
+                b[i - 1][j] *= 2.0
+    # Output layer: only weights[0] of the single output neuron is scaled.
+    W[-1][0][0] *= 0.5
+    conn = []
+    for Wl, bl in zip(W, b):
+        for jin in range(Wl.shape[1]):
+            for k in range(Wl.shape[0]):
+                conn.append(Wl[k, jin])
+        conn.extend(bl.tolist())
+    return np.array(conn)
+
+
+def write_weights(d, nsf, nodes, acts, seed):
+    for e, z in ((0, 1), (1, 8)):
+        rng = np.random.default_rng(seed + e)
+        c = nguyen_widrow([nsf] + list(nodes) + [1], acts, rng)
+        with open(os.path.join(d, f"weights.{z:03d}.data"), "w") as f:
+            f.write("# Seeded U[-1,1] + Nguyen-Widrow; setConnections order\n")
+            for v in c:
+                f.write(f"{v:24.16E}\n")
+
+
+def write_scaling(d, n_frames=10, n_mol=64):
+    ref = RefModel(d, unscaled=True)
+    ne = ref.num_elements
+    vals = [[] for _ in range(ne)]
+    for f in range(n_frames):
+        box, pos, elem = synth.water_box(n_mol, seed=1000 + f)
+        ref.set_structure(pos, elem, box)
+        ref.evaluate(False)
+        G = ref.G()
+        for e in range(ne):
+            vals[e].append(G[elem == e, :ref.num_sf[e]])
+    with open(os.path.join(d, "scaling.data"), "w") as f:
+        f.write("#" + "#" * 80 + "\n")
+        f.write("# Symmetry function scaling data (unscaled SF statistics "
+                f"over {n_frames} water boxes of {n_mol} molecules).\n")
+        f.write("# e_index sf_index sf_min sf_max sf_mean sf_sigma\n")
+        f.write("#" + "#" * 80 + "\n")
+        for e in range(ne):
+            a = np.concatenate(vals[e], axis=0)
+            n = a.shape[0]
+            s = a.sum(axis=0)
+            s2 = (a * a).sum(axis=0)
+            for k in range(a.shape[1]):
+                mean = s[k] / n
+                # Two-pass variance: the one-pass form of Dataset.cpp cancels
+                # catastrophically for the narrow zeta = 16 functions.
+                sigma = float(np.std(a[:, k], ddof=1))
+                f.write(f"{e + 1:10d} {k + 1:10d} {a[:, k].min():24.16E} "
+                        f"{a[:, k].max():24.16E} {mean:24.16E} "
+                        f"{sigma:24.16E}\n")
+
+
+def make(name, radial_eta, ang_eta, zetas, nodes, acts, seed):
+    d = os.path.join(OUT, name)
+    os.makedirs(d, exist_ok=True)
+    lines = sf_lines(radial_eta, ang_eta, zetas)
+    write_input_nn(d, nodes, acts, lines)
+    nsf = len(lines) // 2
+    write_weights(d, nsf, nodes, acts, seed)
+    write_scaling(d)
+    print(f"{name}: {nsf} SFs per element -> {d}")
+
+
+if __name__ == "__main__":
+    base_eta = [0.001, 0.01, 0.03, 0.06, 0.15, 0.3, 0.6, 1.5]
+    make("h2o_52", base_eta, [0.001, 0.01, 0.05], [1.0, 4.0],
+         [25, 25], ["t", "t", "l"], seed=52)
+    make("h2o_92", base_eta + [2.5, 4.0], [0.001, 0.01, 0.05],
+         [1.0, 2.0, 4.0, 16.0], [64, 64, 64], ["p", "p", "p", "l"], seed=92)
