@@ -1,0 +1,461 @@
+"""Energy + force throughput of the n2p2 prediction path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload (the FP64 plain form at scale): a periodic water box of 8,192
+molecules = 24,576 atoms at 1.0 g/cm^3 (cubic, L = 118.26 bohr), seeded
+uniform O positions with O-O >= 4.7 bohr, seeded orientations, then 100
+frames with Gaussian position noise sigma = 0.1 bohr.  Potential: 52 symmetry
+functions per element (radial + narrow angular, cos cutoff 12 bohr), NN
+52-25-25-1 (tanh), seeded Nguyen-Widrow weights (tests/golden/potentials/
+h2o_52).  One step = one frame through neighbor list, symmetry functions +
+dG/dr, atomic NNs + dE/dG, energy and forces, all in FP64.
+
+Metric: E+F atoms/s (higher is better).
+  value : device-resident frames (HBM), K steps between CUDA events on the
+          library's stream, max over ranks; frames cycle through 100
+          distinct coordinate sets and the per-frame working set (dG/dr,
+          2 GB) is far larger than L2.
+  e2e   : the same through the C-ABI with HOST buffers -- every step copies
+          the frame's positions host->device (pinned) and reads back energy
+          and forces (n2p2b_set_positions / n2p2b_evaluate /
+          n2p2b_get_forces / n2p2b_get_energy), wall clock around K steps.
+
+Multi-GPU: one process per GPU (torchrun); each rank evaluates its own
+frames (independent replicas, weak scaling, no data-path collective); the
+time is the max over ranks.
+
+--impl reference times the reference n2p2 CPU path (oracle/_ref, OpenMP on
+all host cores) on the same workload; each step is one full frame.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+POT = os.path.join(ROOT, "tests", "golden", "potentials", "h2o_52")
+N_MOL = 8192
+SEED = 2026
+N_FRAMES = 100
+SIGMA = 0.1
+METRIC = "E+F atoms/s (plain FP64, 24,576-atom water box)"
+
+
+def args():
+    a = argparse.ArgumentParser()
+    a.add_argument("--gpus", type=int, default=1)
+    a.add_argument("--steps", type=int, default=200)
+    a.add_argument("--warmup", type=int, default=5)
+    a.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    a.add_argument("--frames", type=int, default=N_FRAMES)
+    a.add_argument("--no-cpu-baseline", action="store_true")
+    return a.parse_args()
+
+
+def workload(rank: int, n_frames: int):
+    from n2p2_b200 import synth
+    box, pos, elem = synth.water_box(N_MOL, SEED)
+    boxes, frames = synth.noisy_frames(pos, n_frames, SIGMA,
+                                       seed=SEED + 1 + 1000 * rank, box=box)
+    return box, frames, elem
+
+
+def config(n_gpus: int, steps_note: str = ""):
+    return {
+        "workload": "water box, 8,192 molecules = 24,576 atoms, 1.0 g/cm^3, "
+                    "L = 118.26 bohr, 100 noisy frames (sigma 0.1 bohr)",
+        "potential": "h2o_52: 52 SFs/element (16 radial G2 + 36 narrow "
+                     "angular G3, cos cutoff rc = 12 bohr), NN 52-25-25-1 tanh",
+        "form": "plain FP64",
+        "atoms_per_step_per_gpu": 3 * N_MOL,
+        "l2": "per-frame working set > L2 (dG/dr buffer ~2 GB; frames cycle)",
+        "parallelism": f"replicas x{n_gpus}",
+        **({"note": steps_note} if steps_note else {}),
+    }
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                 "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx.append(float(f[1]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [],
+                    "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work model (FLOPs and bytes per frame)
+# ---------------------------------------------------------------------------
+def work_model(cnt, index, dr, d, elem, rc=12.0):
+    """Exact neighbor (n) and valid-triplet (T) counts of one frame and the
+    FLOP / byte model: per triplet 40 + 60 M_a, per (pair, radial member)
+    20, NN 3*2*MAC, chain rule 6 per stored Vec3D slot; bytes of the SF
+    kernel = neighbor data read + dG/dr, G and dG/dr(self) written."""
+    import torch
+    dev = torch.device("cuda")
+    N = len(cnt)
+    off = np.concatenate([[0], np.cumsum(cnt)])
+    mx = int(cnt.max())
+    # padded [atom, neighbor, xyz]; padding sits far outside the cutoff
+    pad = np.full((N, mx, 3), 1e6)
+    valid = np.zeros((N, mx), dtype=bool)
+    for i in range(N):
+        k = int(cnt[i])
+        pad[i, :k] = dr[off[i]:off[i + 1]]
+        valid[i, :k] = d[off[i]:off[i + 1]] < rc
+    pad[~valid] = 1e6
+    T = 0
+    rc2 = rc * rc
+    tri = torch.triu(torch.ones(mx, mx, dtype=torch.bool, device=dev), 1)
+    for b in range(0, N, 1024):
+        v = torch.tensor(pad[b:b + 1024], device=dev)
+        ok = torch.tensor(valid[b:b + 1024], device=dev)
+        dd = ((v[:, :, None, :] - v[:, None, :, :]) ** 2).sum(-1)
+        m = (dd < rc2) & ok[:, :, None] & ok[:, None, :] & tri
+        T += int(m.sum())
+    n = int(cnt.sum())
+    M_a, M_r, S, n_sf = 12, 8, 32, 52
+    mac = 52 * 25 + 25 * 25 + 25
+    flops_sf = T * (40 + 60 * M_a) + n * M_r * 20
+    flops_all = flops_sf + N * 3 * 2 * mac + 6 * (n * S + N * n_sf)
+    bytes_sf = n * 32 + n * S * 3 * 8 + N * n_sf * 8 * 4 + N * 8 * 2
+    return {"atoms": N, "neighbors": n, "triplets": T,
+            "neighbors_per_atom": n / N, "triplets_per_atom": T / N,
+            "flops_sf": flops_sf, "flops_total": flops_all,
+            "bytes_sf": bytes_sf}
+
+
+def fp64_peak_tflops():
+    """Dense FP64 peak measured here: cuBLAS DGEMM 8192^3 via torch (best
+    of 5).  The plain FP64 kernels run on the FP64 pipe."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    b = torch.randn(n, n, dtype=torch.float64, device="cuda")
+    torch.matmul(a, b)
+    torch.cuda.synchronize()
+    best = 1e30
+    for _ in range(5):
+        s = torch.cuda.Event(enable_timing=True)
+        e = torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e) / 1e3)
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / best / 1e12
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            j = json.load(fh)
+        return j.get("hbm_gbs", 6650.0), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline (reference library, OpenMP) -- rank 0, N = 1 only
+# ---------------------------------------------------------------------------
+def cpu_baseline(frames, box, elem, reps=1):
+    from oracle import ref as oref
+    lib = os.path.join(ROOT, "oracle", "_ref", "libn2p2ref_perf.so")
+    if not os.path.exists(lib):
+        return {"value": None, "unit": "atoms/s", "cores": 0,
+                "kind": "reference", "sample": "unavailable: oracle/_ref "
+                "not built"}
+    oref.REF_LIB = lib
+    threads = os.cpu_count() or 1
+    m = oref.RefModel(POT)
+    m.set_structure(frames[0], elem, box)
+    t = m.time_stages(threads=threads, reps=reps)
+    total = float(t.sum())
+    natoms = len(elem) * reps
+    return {"value": natoms / total, "unit": "atoms/s", "cores": threads,
+            "kind": "reference",
+            "sample": f"{reps} frame(s) of the 24,576-atom box, full path "
+                      "(neighbor list + SF + NN + E + F); stage seconds "
+                      f"NL {t[0]:.2f}, SF {t[1]:.2f}, NN {t[2]:.2f}, "
+                      f"E {t[3]:.4f}, F {t[4]:.2f}; without the O(N^2) "
+                      f"neighbor list: {natoms / (total - t[0]):.0f} atoms/s"}
+
+
+def run_reference(a):
+    """--impl reference: the reference CPU path on the same workload."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    from oracle import ref as oref
+    lib = os.path.join(ROOT, "oracle", "_ref", "libn2p2ref_perf.so")
+    if not os.path.exists(lib):
+        print(json.dumps({"impl": "reference",
+                          "unavailable": "oracle/_ref not built here"}))
+        return
+    oref.REF_LIB = lib
+    box, frames, elem = workload(0, min(a.frames, max(a.steps, 1) + 1))
+    threads = os.cpu_count() or 1
+    m = oref.RefModel(POT)
+    # one warm-up frame (a CPU path has no device warm-up to amortize)
+    m.set_structure(frames[0], elem, box)
+    t0 = time.perf_counter()
+    m.time_stages(threads=threads, reps=1)
+    per = time.perf_counter() - t0
+    budget = 150.0
+    k = max(1, min(a.steps, int(budget / max(per, 1e-3))))
+    tot = np.zeros(5)
+    for s in range(k):
+        m.set_structure(frames[(s + 1) % len(frames)], elem, box)
+        tot += m.time_stages(threads=threads, reps=1)
+    secs = float(tot.sum())
+    val = len(elem) * k / secs
+    note = "" if k == a.steps else (f"timed {k} of {a.steps} requested steps "
+                                    "(150 s budget; one frame per step)")
+    line = {
+        "metric": METRIC, "value": val, "unit": "atoms/s", "impl": "reference",
+        "n_gpus": a.gpus, "steps": k, "warmup": 1,
+        "ms_per_step": 1e3 * secs / k, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": config(a.gpus, note),
+        "cpu_baseline": {"value": val, "unit": "atoms/s", "cores": threads,
+                         "kind": "reference",
+                         "sample": f"{k} full frame(s) per run, stage "
+                                   f"seconds NL {tot[0]:.2f} SF {tot[1]:.2f} "
+                                   f"NN {tot[2]:.2f} E {tot[3]:.4f} "
+                                   f"F {tot[4]:.2f}"},
+        "e2e": {"value": val, "unit": "atoms/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(a):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(
+            seconds=600), device_id=torch.device("cuda", local))
+
+    from n2p2_b200 import _capi
+    from n2p2_b200.mode import Prediction
+
+    box, frames, elem = workload(rank, a.frames)
+    n = len(elem)
+    F = len(frames)
+    dev_frames = torch.tensor(frames, dtype=torch.float64, device="cuda")
+    host_frames = torch.tensor(frames, dtype=torch.float64).pin_memory()
+    host_forces = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    stream = torch.cuda.Stream()
+
+    p = Prediction(POT, device=local)
+    p.setup()
+    p.set_stream(stream.cuda_stream)
+    p.set_structure(host_frames[0].numpy(), elem, box)
+    p.evaluate_nnp(True)          # sizes all buffers (capacity known)
+    lib = _capi.load()
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- warm-up ---------------------------------------------------------
+    for s in range(max(a.warmup, 3)):
+        p.set_positions(dev_frames[s % F])
+        p.evaluate_async(True)
+    p.finish()
+
+    with ClockSampler(local) as clocks:
+        # ---- value: device-resident frames -------------------------------
+        barrier()
+        l0 = lib.n2p2b_kernel_launch_count()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        for s in range(a.steps):
+            p.set_positions(dev_frames[s % F])
+            p.evaluate_async(True)
+        ev1.record(stream)
+        p.finish()
+        barrier()
+        launches = int(lib.n2p2b_kernel_launch_count() - l0)
+        t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+
+        # ---- e2e: host buffers through the C-ABI -------------------------
+        barrier()
+        t0 = time.perf_counter()
+        energy = 0.0
+        for s in range(a.steps):
+            p.set_positions(host_frames[s % F].numpy())
+            p.evaluate_nnp(True)
+            p._check(lib.n2p2b_get_forces(p._h, host_forces.data_ptr(),
+                                          _capi.HOST))
+            energy = p.energy
+        barrier()
+        t_e2e = max_over_ranks(time.perf_counter() - t0)
+
+        # ---- profiled pass: per-stage device time -------------------------
+        p.set_profiling(True)
+        p.stage_times(reset=True)
+        for s in range(a.steps):
+            p.set_positions(dev_frames[s % F])
+            p.evaluate_async(True)
+        p.finish()
+        stage_ms, runs = p.stage_times(reset=True)
+        p.set_profiling(False)
+
+    if dist is not None:
+        dist.barrier()
+
+    atoms_total = n * a.steps * world
+    value = atoms_total / t_dev
+    e2e = atoms_total / t_e2e
+    if rank != 0:
+        if dist is not None:
+            dist.destroy_process_group()
+        return
+
+    # ---- roofline of the dominant kernel (symmetry functions) -------------
+    p.set_positions(dev_frames[0])
+    p.evaluate_nnp(True)
+    cnt, index, dr, d = p.neighbor_list()
+    wm = work_model(cnt, index, dr, d, elem)
+    per = [x / max(runs, 1) for x in stage_ms]
+    sf_s = per[1] / 1e3
+    hbm_peak, peak_kind = measured_peaks()
+    gbs = wm["bytes_sf"] / sf_s / 1e9
+    fp64_peak = fp64_peak_tflops()
+    sf_tflops = wm["flops_sf"] / sf_s / 1e12
+
+    line = {
+        "metric": METRIC,
+        "value": value, "unit": "atoms/s",
+        "n_gpus": world, "steps": a.steps, "warmup": max(a.warmup, 3),
+        "ms_per_step": 1e3 * t_dev / a.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic", "config": config(world),
+        "e2e": {"value": e2e, "unit": "atoms/s",
+                "h2d_bytes_per_step": n * 3 * 8,
+                "d2h_bytes_per_step": n * 3 * 8 + 8,
+                "path": "n2p2b_set_positions(host) + n2p2b_evaluate + "
+                        "n2p2b_get_forces(host) + n2p2b_get_energy"},
+        "gpu_launches": launches,
+        "stage_ms_per_step": {"neighbor_list": per[0],
+                              "symmetry_functions": per[1],
+                              "neural_networks": per[2], "energy": per[3],
+                              "forces": per[4]},
+        "roofline": {"kernel": "sfFp64Kernel (symmetry functions + dG/dr)",
+                     "bound": "hbm", "achieved": gbs, "peak": hbm_peak,
+                     "unit": "GB/s", "frac": gbs / hbm_peak,
+                     "peak_source": peak_kind,
+                     "traffic": None,
+                     "algorithmic_bytes_per_launch": wm["bytes_sf"]},
+        "roofline_fp64": {"kernel": "sfFp64Kernel", "achieved": sf_tflops,
+                          "peak": fp64_peak, "unit": "TFLOP/s",
+                          "frac": sf_tflops / fp64_peak,
+                          "peak_source": "cuBLAS DGEMM 8192^3 measured here",
+                          "algorithmic_flops_per_launch": wm["flops_sf"]},
+        "work": wm,
+        "energy_last_frame": energy,
+        "clocks": clocks.summary(),
+    }
+    if not a.no_cpu_baseline and world == 1:
+        line["cpu_baseline"] = cpu_baseline(frames, box, elem)
+    print(json.dumps(line))
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+def main():
+    a = args()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)
+
+
+if __name__ == "__main__":
+    main()

@@ -51,7 +51,9 @@ typedef struct n2p2b_context n2p2b_context;
 /* ---- context ---------------------------------------------------------- */
 
 /* Creates a context on CUDA device `device`.  Replaces constructing
- * nnp::Mode / nnp::Prediction (libnnp/Mode.h:86, Prediction.h:27). */
+ * nnp::Mode / nnp::Prediction (libnnp/Mode.h:86, Prediction.h:27).
+ * device = -1 creates a host-only context: setup and potential queries work,
+ * evaluation calls return N2P2B_ERR_STATE. */
 int         n2p2b_create(int device, n2p2b_context** ctx);
 void        n2p2b_destroy(n2p2b_context* ctx);
 const char* n2p2b_last_error(const n2p2b_context* ctx);
@@ -91,6 +93,18 @@ int    n2p2b_num_symmetry_functions(const n2p2b_context* ctx, int e);
 int    n2p2b_num_slots(const n2p2b_context* ctx, int e, int ne);
 /* Mode::getMaxCutoffRadius (normalized units, libnnp/Mode.h:693). */
 double n2p2b_max_cutoff_radius(const n2p2b_context* ctx);
+/* Parameters of symmetry function s (sorted index = NN input index) of
+ * element e, as Element::getSymmetryFunction(s) holds them (normalized
+ * units): out[0..9] = type, e1, e2 (-1 for radial), eta, rs, rc, zeta,
+ * lambda, scaling factor, input.nn line number (0-based). */
+int    n2p2b_symmetry_function_params(const n2p2b_context* ctx, int e, int s,
+                                      double* out);
+/* Element::setupSymmetryFunctionGroups: number of groups of element e and
+ * the SF indices of group g's members in member order (returns the member
+ * count; writes at most cap indices). */
+int    n2p2b_num_groups(const n2p2b_context* ctx, int e);
+int    n2p2b_group_members(const n2p2b_context* ctx, int e, int g,
+                           int32_t* idx, int cap);
 
 /* ---- structure (nnp::Structure) --------------------------------------- */
 
@@ -155,6 +169,19 @@ int n2p2b_get_dEdG(n2p2b_context* ctx, double* dEdG, int stride);
  * [3], entries in n2p2b_get_neighbor_list order). */
 int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sf_stride,
                    double* neighbor, int slot_stride);
+
+/* ---- diagnostics (no counterpart in the reference) -------------------- */
+
+/* Records CUDA events around each stage of every following evaluation on
+ * the context's stream (device time; no host synchronization added). */
+int n2p2b_set_profiling(n2p2b_context* ctx, int enable);
+/* Summed device milliseconds per stage since the last reset: ms[0..4] =
+ * neighbor list, symmetry functions, atomic NNs, energy, forces; *runs =
+ * number of profiled evaluations.  Synchronizes the context's stream. */
+int n2p2b_get_stage_times(n2p2b_context* ctx, double* ms, int64_t* runs,
+                          int reset);
+/* Number of kernel launches this library has issued in this process. */
+uint64_t n2p2b_kernel_launch_count(void);
 
 /* ---- one call per frame ----------------------------------------------- */
 

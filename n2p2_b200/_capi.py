@@ -45,6 +45,9 @@ SIGNATURES = {
     "n2p2b_num_symmetry_functions": (C.c_int, [_vp, C.c_int]),
     "n2p2b_num_slots": (C.c_int, [_vp, C.c_int, C.c_int]),
     "n2p2b_max_cutoff_radius": (C.c_double, [_vp]),
+    "n2p2b_symmetry_function_params": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
+    "n2p2b_num_groups": (C.c_int, [_vp, C.c_int]),
+    "n2p2b_group_members": (C.c_int, [_vp, C.c_int, C.c_int, _i32p, C.c_int]),
     "n2p2b_set_structure": (C.c_int, [_vp, C.c_int64, _vp, _vp, C.c_int,
                                       _i32p, C.c_int]),
     "n2p2b_set_positions": (C.c_int, [_vp, _vp, C.c_int]),
@@ -65,6 +68,9 @@ SIGNATURES = {
     "n2p2b_get_dEdG": (C.c_int, [_vp, _dp, C.c_int]),
     "n2p2b_get_dGdr": (C.c_int, [_vp, _dp, C.c_int, _dp, C.c_int]),
     "n2p2b_predict": (C.c_int, [_vp, C.c_int64, _vp, _vp, _i32p, _dp, _dp]),
+    "n2p2b_set_profiling": (C.c_int, [_vp, C.c_int]),
+    "n2p2b_get_stage_times": (C.c_int, [_vp, _dp, _i64p, C.c_int]),
+    "n2p2b_kernel_launch_count": (C.c_uint64, []),
 }
 
 _lib = None
@@ -75,7 +81,7 @@ def load(path: str | None = None):
     global _lib
     if _lib is not None and path is None:
         return _lib
-    p = path or LIB_PATH
+    p = path or os.environ.get("N2P2B_LIBRARY") or LIB_PATH
     if not os.path.exists(p):
         raise ImportError(
             f"{p} is missing: build it with `python -m n2p2_b200.build` "

@@ -9,6 +9,7 @@
 #include "potential.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -151,7 +152,22 @@ __global__ void statusResetKernel(int* status)
     if (threadIdx.x == ST_BAD_ATOM) status[threadIdx.x] = -1;
 }
 
+std::atomic<unsigned long long> g_launches{0};
+
+// Stage boundaries of one profiled pipeline run: events before NL and after
+// NL, SF, NN, energy and forces (stages not run record nothing).
+struct StageEvents
+{
+    cudaEvent_t ev[6];
+    bool        used[6];
+};
+
 } // namespace
+
+namespace n2p2b
+{
+void noteLaunches(int k) { g_launches += (unsigned long long)k; }
+} // namespace n2p2b
 
 struct n2p2b_context
 {
@@ -191,17 +207,84 @@ struct n2p2b_context
     DevBuf       G, dEdG, dGdrSelf, Ei, selfF, F, energyOut, status;
     int*         statusHost = nullptr;
     double*      energyHost = nullptr;
-    int          sfCap = 256;
+    int          sfCap = 0;      // 0 = size from the next neighbor list
+    int          lastMaxNbr = 0; // largest neighbor count of the last list
     int          sfGrid = 0;
     int          sfGridCap = 0;
+    int          sfVariant = -1;  // chosen from the potential's groups
+    int          sfSortCats = 0;
     int          smCount = 0;
 
     // Pipeline state (what the last calls computed).
     bool haveNL = false, haveSF = false, haveSFDeriv = false, haveNN = false;
     bool haveNNDeriv = false, haveE = false, haveF = false;
 
+    // Per-stage device timing (n2p2b_set_profiling).
+    bool                     profiling = false;
+    std::vector<StageEvents> pendingEvents;
+    std::vector<StageEvents> freeEvents;
+    double                   stageMs[5] = {0, 0, 0, 0, 0};
+    long                     stageRuns = 0;
+    StageEvents*             cur = nullptr;
+
+    void mark(int k)
+    {
+        if (!cur) return;
+        ck(cudaEventRecord(cur->ev[k], stream), "cudaEventRecord");
+        cur->used[k] = true;
+    }
+
+    void beginProfile()
+    {
+        if (!profiling) return;
+        StageEvents se;
+        if (!freeEvents.empty())
+        {
+            se = freeEvents.back();
+            freeEvents.pop_back();
+        }
+        else
+        {
+            for (auto& e : se.ev) ck(cudaEventCreate(&e), "cudaEventCreate");
+        }
+        for (auto& u : se.used) u = false;
+        pendingEvents.push_back(se);
+        cur = &pendingEvents.back();
+        mark(0);
+    }
+
+    void endProfile() { cur = nullptr; }
+
+    // Synchronizes and folds all pending events into stageMs.
+    void collectProfile()
+    {
+        if (pendingEvents.empty()) return;
+        ck(cudaStreamSynchronize(stream), "synchronize");
+        for (auto& se : pendingEvents)
+        {
+            int prev = 0;
+            for (int k = 1; k < 6; ++k)
+            {
+                if (!se.used[k]) continue;
+                float ms = 0.0f;
+                ck(cudaEventElapsedTime(&ms, se.ev[prev], se.ev[k]),
+                   "cudaEventElapsedTime");
+                stageMs[k - 1] += ms;
+                prev = k;
+            }
+            ++stageRuns;
+            freeEvents.push_back(se);
+        }
+        pendingEvents.clear();
+    }
+
     ~n2p2b_context()
     {
+        if (stream) cudaStreamSynchronize(stream);
+        for (auto& se : pendingEvents)
+            for (auto& e : se.ev) cudaEventDestroy(e);
+        for (auto& se : freeEvents)
+            for (auto& e : se.ev) cudaEventDestroy(e);
         for (DevBuf* b : {&sfScale, &nnW, &slotSF, &posIn, &pos, &elem,
                           &atomsByElem, &cellOf, &cellCount, &cellFill,
                           &cellStart, &cellAtoms, &cellStatus, &nbrCount,
@@ -215,12 +298,51 @@ struct n2p2b_context
         if (ownStream && stream) cudaStreamDestroy(stream);
     }
 
-    void activate() { ck(cudaSetDevice(device), "cudaSetDevice"); }
+    // Host-only contexts (device < 0) support setup and potential queries.
+    bool hostOnly() const { return device < 0; }
+
+    void activate()
+    {
+        if (hostOnly())
+            throw StateError("ERROR: This context has no CUDA device (it was "
+                             "created with device -1 for setup only).\n");
+        ck(cudaSetDevice(device), "cudaSetDevice");
+    }
 
     // ---- potential tables ------------------------------------------------
 
+    // Number of (zeta, lambda) shapes if the angular group's members are
+    // (eta runs) x shapes -- each run has the same shape list, zeta is
+    // integer, rs = 0 -- else 0.  Members are sorted with eta slowest
+    // (SymGrpExpAngn::sortMembers), so runs are contiguous.
+    static int productShapes(Element const& el, SymGrp const& g)
+    {
+        std::size_t const M = g.members.size();
+        if (M == 0) return 0;
+        SymFnc const& f0 = el.sfs[g.members[0]];
+        std::size_t ns = 0;
+        while (ns < M && el.sfs[g.members[ns]].eta == f0.eta) ++ns;
+        if (ns == 0 || ns > 8 || M % ns != 0) return 0;
+        for (std::size_t r = 0; r < M / ns; ++r)
+        {
+            double const eta = el.sfs[g.members[r * ns]].eta;
+            if (r > 0 && eta == el.sfs[g.members[(r - 1) * ns]].eta) return 0;
+            for (std::size_t s = 0; s < ns; ++s)
+            {
+                SymFnc const& f = el.sfs[g.members[r * ns + s]];
+                SymFnc const& b = el.sfs[g.members[s]];
+                if (f.eta != eta || f.rs != 0.0 || !f.useIntegerPow
+                    || f.zeta != b.zeta || f.lambda != b.lambda)
+                    return 0;
+            }
+        }
+        return (int)ns;
+    }
+
     void buildTables()
     {
+        sfVariant = -1;
+        sfGrid = 0;
         int const ne = pot.numElements();
         if (ne > kMaxElem)
             throw std::runtime_error("ERROR: More elements than the device "
@@ -243,10 +365,12 @@ struct n2p2b_context
         std::vector<int16_t> slotTab((std::size_t)kMaxElem * kMaxElem
                                      * std::max(maxSlots, 1), (int16_t)-1);
         int gi = 0, mi = 0;
+        sfp.maxExp = 1;
         for (int e = 0; e < ne; ++e)
         {
             Element const& el = pot.elements[e];
             sfp.groupBeg[e] = gi;
+            int expCount = 0;
             sfp.numSF[e] = (int)el.sfs.size();
             for (int f = 0; f < ne; ++f)
             {
@@ -310,6 +434,8 @@ struct n2p2b_context
                             ? &el.sfs[g.members[k - 1]] : nullptr;
                         m.calcExp = (prev == nullptr || prev->eta != s.eta
                                      || prev->rs != s.rs) ? 1 : 0;
+                        if (m.calcExp) ++expCount;
+                        m.expIdx = (int16_t)(expCount - 1);
                         q.q = m.factorNorm / s.scalingFactor;
                     }
                     switch (s.scalingType)
@@ -324,7 +450,9 @@ struct n2p2b_context
                                          q.shift = s.Gmean; break;
                     }
                 }
+                d.shapes = (g.type == 2) ? 0 : productShapes(el, g);
             }
+            sfp.maxExp = std::max(sfp.maxExp, expCount);
         }
         sfp.groupBeg[ne] = gi;
 
@@ -363,6 +491,11 @@ struct n2p2b_context
             throw std::runtime_error("ERROR: NN layer wider than supported.\n");
         nnp.maxWidth = maxW;
 
+        if (hostOnly())
+        {
+            tablesReady = true;
+            return;
+        }
         activate();
         sfScale.ensure(sizeof(SFScale) * scale.size());
         ck(cudaMemcpy(sfScale.p, scale.data(), sizeof(SFScale) * scale.size(),
@@ -415,6 +548,8 @@ struct n2p2b_context
         }
         activate();
         n = num;
+        sfCap = 0;
+        lastMaxNbr = 0;
         elemHost.assign(elems, elems + num);
         periodic = box != nullptr;
         remap = periodic && (flags & N2P2B_REMAP);
@@ -565,6 +700,7 @@ struct n2p2b_context
 
     void enqueueReset()
     {
+        noteLaunches(2);
         statusResetKernel<<<1, 32, 0, stream>>>(status.as<int>());
         statusResetKernel<<<1, 32, 0, stream>>>(cellStatus.as<int>());
     }
@@ -611,19 +747,32 @@ struct n2p2b_context
 
     void enqueueSF(bool deriv)
     {
+        if (sfVariant < 0)
+        {
+            sfVariant = sfDefaultVariant(sfp);
+            if (char const* v = std::getenv("N2P2B_SF_VARIANT"))
+                sfVariant = std::atoi(v);
+            sfSortCats = 1;
+            if (char const* v = std::getenv("N2P2B_SF_SORT"))
+                sfSortCats = std::atoi(v);
+        }
         if (sfGrid == 0 || sfGridCap != sfCap)
         {
             ck(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount,
                                       device), "device attribute");
-            sfGrid = smCount * sfBlocksPerSM(sfp, sfCap);
+            sfGrid = smCount * sfBlocksPerSM(sfp, sfCap, sfVariant);
             sfGridCap = sfCap;
         }
+        long const blocksNeeded = (n + sfAtomsPerBlock() - 1)
+                                / sfAtomsPerBlock();
         SFLaunch L;
         L.n = (int)n;
         L.derivatives = deriv ? 1 : 0;
         L.cap = sfCap;
         L.memberChunk = 12;
-        L.grid = (int)std::min<long>(sfGrid, n);
+        L.grid = (int)std::max<long>(1, std::min<long>(sfGrid, blocksNeeded));
+        L.variant = sfVariant;
+        L.sortCats = sfSortCats;
         L.elem = elem.as<int>();
         L.nbrOff = nbrOff.as<int>();
         L.nbrCountElem = nbrCountElem.as<int>();
@@ -719,6 +868,18 @@ struct n2p2b_context
     }
 
     // Runs `stages` (bit 0 NL, 1 SF, 2 NN, 3 E, 4 F) with capacity retries.
+    // Staging capacity of the SF kernel: the largest neighbor count plus
+    // headroom for the next frames, in multiples of 32.
+    void fitSFCap(int maxNbr)
+    {
+        maxNbr = std::max(maxNbr, lastMaxNbr);
+        int const cap = ((std::max(maxNbr, 1) + 8 + 15) / 16) * 16;
+        if (sfSharedBytes(sfp, cap) > 227 * 1024)
+            throw CapacityError("ERROR: An atom has more neighbors than the "
+                                "symmetry-function kernel can stage.\n");
+        sfCap = std::max(cap, sfCap);
+    }
+
     void run(int stages, bool sfDeriv, bool nnDeriv)
     {
         requireReady();
@@ -726,41 +887,48 @@ struct n2p2b_context
         activate();
         ensureStructureBuffers();
         ensureEntryBuffers();
-        for (int attempt = 0; attempt < 6; ++attempt)
+        for (int attempt = 0; attempt < 8; ++attempt)
         {
             enqueueReset();
             int st = stages;
-            // Later stages need the neighbor list of this run.
-            if (st & 1) enqueueNL();
-            if (st & 2) enqueueSF(sfDeriv);
-            if (st & 4) enqueueNN(nnDeriv);
-            if (st & 8) enqueueEnergy();
-            if (st & 16) enqueueForces();
+            // Unknown neighbor counts (new structure): run the neighbor list
+            // alone first and size the SF staging from its maximum.
+            bool const sizing = (st & 1) && (st & 2) && sfCap <= 0;
+            if (sizing) st = 1;
+            beginProfile();
+            if (st & 1) { enqueueNL(); mark(1); }
+            if (st & 2) { enqueueSF(sfDeriv); mark(2); }
+            if (st & 4) { enqueueNN(nnDeriv); mark(3); }
+            if (st & 8) { enqueueEnergy(); mark(4); }
+            if (st & 16) { enqueueForces(); mark(5); }
+            endProfile();
             checkLaunch("kernel launch");
             int const flags = readStatus();
+            if (st & 1) lastMaxNbr = statusHost[ST_MAX_NBR];
             if (flags & FLAG_NBR_OVERFLOW)
             {
                 grow(statusHost[ST_TOTAL_NBR]);
                 stages |= 1;
                 continue;
             }
-            if (flags & FLAG_SF_CAPACITY)
-            {
-                int const need = statusHost[ST_MAX_NBR] > 0
-                               ? statusHost[ST_MAX_NBR] : sfCap * 2;
-                int const cap = ((need + 31) / 32) * 32;
-                std::size_t const shm = sfSharedBytes(sfp, cap);
-                if (shm > 227 * 1024)
-                    throw CapacityError("ERROR: An atom has more neighbors "
-                                        "than the symmetry-function kernel "
-                                        "can stage.\n");
-                sfCap = std::max(cap, sfCap + 32);
-                continue;
-            }
             if (flags & FLAG_MIRROR_MISSING)
                 throw std::runtime_error("ERROR: Internal: neighbor list is "
                                          "not symmetric.\n");
-            if (stages & 1) haveNL = true;
+            if (sizing || (flags & FLAG_SF_CAPACITY))
+            {
+                fitSFCap(statusHost[ST_MAX_NBR]);
+                if (sizing)
+                {
+                    haveNL = true;
+                    stages &= ~1;   // the neighbor list of this run stands
+                }
+                continue;
+            }
+            if (stages & 1)
+            {
+                haveNL = true;
+                if (sfCap <= 0) fitSFCap(lastMaxNbr);
+            }
             if (stages & 2) { haveSF = true; haveSFDeriv = sfDeriv; }
             if (stages & 4) { haveNN = true; haveNNDeriv = nnDeriv; }
             if (stages & 8) haveE = true;
@@ -779,11 +947,21 @@ struct n2p2b_context
             throw StateError("ERROR: evaluate_async needs known capacities: "
                              "run n2p2b_evaluate once first.\n");
         enqueueReset();
+        beginProfile();
         enqueueNL();
+        mark(1);
         enqueueSF(forces);
+        mark(2);
         enqueueNN(forces);
+        mark(3);
         enqueueEnergy();
-        if (forces) enqueueForces();
+        mark(4);
+        if (forces)
+        {
+            enqueueForces();
+            mark(5);
+        }
+        endProfile();
         checkLaunch("kernel launch");
     }
 
@@ -884,6 +1062,13 @@ int n2p2b_create(int device, n2p2b_context** out)
 {
     if (out == nullptr) return N2P2B_ERR_ARGUMENT;
     *out = nullptr;
+    if (device == -1)
+    {
+        n2p2b_context* c = new n2p2b_context();
+        c->device = -1;
+        *out = c;
+        return N2P2B_OK;
+    }
     int count = 0;
     if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0
         || device >= count)
@@ -905,9 +1090,43 @@ int n2p2b_create(int device, n2p2b_context** out)
 void n2p2b_destroy(n2p2b_context* ctx)
 {
     if (ctx == nullptr) return;
-    cudaSetDevice(ctx->device);
-    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (!ctx->hostOnly())
+    {
+        cudaSetDevice(ctx->device);
+        if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    }
     delete ctx;
+}
+
+int n2p2b_symmetry_function_params(n2p2b_context const* ctx, int e, int s,
+                                   double* out)
+{
+    if (!ctx || !out || e < 0 || e >= ctx->pot.numElements()) return N2P2B_ERR_ARGUMENT;
+    Element const& el = ctx->pot.elements[e];
+    if (s < 0 || s >= (int)el.sfs.size()) return N2P2B_ERR_ARGUMENT;
+    SymFnc const& f = el.sfs[s];
+    double const v[10] = {(double)f.type, (double)f.e1, (double)f.e2, f.eta,
+                          f.rs, f.rc, f.zeta, f.lambda, f.scalingFactor,
+                          (double)f.lineNumber};
+    for (int k = 0; k < 10; ++k) out[k] = v[k];
+    return N2P2B_OK;
+}
+
+int n2p2b_num_groups(n2p2b_context const* ctx, int e)
+{
+    if (!ctx || e < 0 || e >= ctx->pot.numElements()) return 0;
+    return (int)ctx->pot.elements[e].groups.size();
+}
+
+int n2p2b_group_members(n2p2b_context const* ctx, int e, int g, int32_t* idx,
+                        int cap)
+{
+    if (!ctx || e < 0 || e >= ctx->pot.numElements()) return N2P2B_ERR_ARGUMENT;
+    auto const& gs = ctx->pot.elements[e].groups;
+    if (g < 0 || g >= (int)gs.size()) return N2P2B_ERR_ARGUMENT;
+    int const m = (int)gs[g].members.size();
+    for (int k = 0; k < m && k < cap; ++k) idx[k] = gs[g].members[k];
+    return m;
 }
 
 char const* n2p2b_last_error(n2p2b_context const* ctx)
@@ -1317,6 +1536,37 @@ int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sfStride,
             }
         }
     });
+}
+
+int n2p2b_set_profiling(n2p2b_context* ctx, int enable)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        ctx->collectProfile();
+        ctx->profiling = enable != 0;
+    });
+}
+
+int n2p2b_get_stage_times(n2p2b_context* ctx, double* ms, int64_t* runs,
+                          int reset)
+{
+    return guarded(ctx, [&] {
+        if (!ms) throw std::invalid_argument("ERROR: ms");
+        ctx->activate();
+        ctx->collectProfile();
+        for (int k = 0; k < 5; ++k) ms[k] = ctx->stageMs[k];
+        if (runs) *runs = ctx->stageRuns;
+        if (reset)
+        {
+            for (double& v : ctx->stageMs) v = 0.0;
+            ctx->stageRuns = 0;
+        }
+    });
+}
+
+uint64_t n2p2b_kernel_launch_count(void)
+{
+    return (uint64_t)g_launches.load();
 }
 
 int n2p2b_predict(n2p2b_context* ctx, int64_t num_atoms, double const* box,

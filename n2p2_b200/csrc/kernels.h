@@ -53,6 +53,9 @@ struct NLLaunch
     int*                status = nullptr;
 };
 
+// Running count of kernel launches issued by this library (diagnostics).
+void noteLaunches(int k);
+
 void launchNeighborList(NLLaunch const& L, cudaStream_t s);
 
 // Symmetry functions (+ derivatives), FP64.
@@ -63,6 +66,9 @@ struct SFLaunch
     int            cap = 0;           // neighbor staging capacity per atom
     int            memberChunk = 12;  // members per register chunk
     int            grid = 0;          // persistent grid size
+    long           warpDoubles = 0;   // shared memory per warp (set by launcher)
+    int            variant = 0;       // product-form shape / run chunking
+    int            sortCats = 0;      // order work categories by partners
     int const*     elem = nullptr;
     int const*     nbrOff = nullptr;
     int const*     nbrCountElem = nullptr;
@@ -80,7 +86,12 @@ struct SFLaunch
 void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L,
                              cudaStream_t s);
 std::size_t sfSharedBytes(SFParams const& P, int cap);
-int sfBlocksPerSM(SFParams const& P, int cap);
+long sfWarpDoubles(SFParams const& P, int cap);
+int sfBlocksPerSM(SFParams const& P, int cap, int variant);
+int sfAtomsPerBlock();
+// Kernel variant matching the potential's product-form groups:
+// 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
+int sfDefaultVariant(SFParams const& P);
 
 // Atomic neural networks (forward + dE/dG), FP64.
 struct NNLaunch

@@ -559,6 +559,7 @@ void launchNeighborList(NLLaunch const& L, cudaStream_t s)
                                             L.status);
     long const cap = L.capacity;
     int const gE = (int)((cap + tb - 1) / tb);
+    noteLaunches(cellEligible ? 11 : 7);
     nlMirrorKernel<<<gE > 0 ? gE : 1, tb, 0, s>>>(
         n, L.p.nimg, L.elem, L.nbrOff, L.key, L.nbrIdx,
         L.entryAtom, L.mirror, L.status);

@@ -315,6 +315,7 @@ void launchNeuralNetworks(NNParams const& P, NNLaunch const& L,
                          cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)shm);
     int const grid = (L.n + kNNWarps - 1) / kNNWarps;
+    noteLaunches(1);
     nnFp64Kernel<<<grid > 0 ? grid : 1, 32 * kNNWarps, shm, s>>>(P, L);
 }
 
@@ -323,6 +324,7 @@ void launchForces(ForceLaunch const& L, cudaStream_t s)
     int const warps = 4;
     std::size_t const shm = sizeof(double) * warps * (std::size_t)L.maxSF;
     int const grid = (L.n + warps - 1) / warps;
+    noteLaunches(2);
     pairForceKernel<<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
     int const tb = 128;
     gatherForceKernel<<<(L.n + tb - 1) / tb > 0 ? (L.n + tb - 1) / tb : 1, tb,
@@ -331,6 +333,7 @@ void launchForces(ForceLaunch const& L, cudaStream_t s)
 
 void launchEnergy(EnergyLaunch const& L, cudaStream_t s)
 {
+    noteLaunches(1);
     energyKernel<<<1, 1024, 0, s>>>(L);
 }
 

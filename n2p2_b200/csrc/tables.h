@@ -22,7 +22,9 @@ struct DevGroup
     int    type;        // 2, 3, 9
     int    e1, e2;      // neighbor elements (e2 == -1: radial)
     int    mbeg, mcnt;  // member range
-    int    pad;
+    int    shapes;      // angular product form: members = runs x shapes
+                        // (same (zeta, lambda) list per eta run, integer
+                        // zeta, rs = 0); 0 = not of that form
     double rc, rc2;     // cutoff radius and its square
     double rci, iw;     // CutoffFunction::rci, iw  (alpha-shifted inner cutoff)
     double rcinv;       // 1 / rc
@@ -43,6 +45,7 @@ struct DevMember
     uint8_t rsPositive;
     uint8_t pad;
     int16_t slot[kMaxElem];  // dG/dr slot per neighbor element, -1 = none
+    int16_t expIdx;       // per-element index of the member's (eta, rs) run
 };
 
 struct SFParams
@@ -51,6 +54,7 @@ struct SFParams
     int       cutoffType;      // CutoffType (global in n2p2)
     int       maxSlots;        // dG/dr slots per neighbor entry (stride)
     int       maxSF;           // SF stride of per-atom arrays
+    int       maxExp;          // max (eta, rs) runs of angular members/element
     int       groupBeg[kMaxElem + 1];
     int       numSF[kMaxElem];
     int       numSlots[kMaxElem][kMaxElem];

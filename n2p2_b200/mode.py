@@ -128,6 +128,24 @@ class Mode:
     def get_max_cutoff_radius(self) -> float:
         return self._L.n2p2b_max_cutoff_radius(self._h)
 
+    def symmetry_function_params(self, e: int, s: int):
+        """type, e1, e2, eta, rs, rc, zeta, lambda, scaling factor, line
+        (Element::getSymmetryFunction(s), normalized units)."""
+        out = (C.c_double * 10)()
+        self._check(self._L.n2p2b_symmetry_function_params(self._h, e, s, out))
+        return np.array(out[:])
+
+    def symmetry_function_groups(self, e: int):
+        """Member SF indices of every group of element e, in group order."""
+        out = []
+        for g in range(self._L.n2p2b_num_groups(self._h, e)):
+            buf = (C.c_int32 * 256)()
+            m = self._L.n2p2b_group_members(self._h, e, g, buf, 256)
+            if m < 0:
+                raise ValueError("bad group")
+            out.append(list(buf[:m]))
+        return out
+
     def element_indices(self, symbols) -> np.ndarray:
         m = {s: i for i, s in enumerate(self.elements)}
         return np.array([m[s] for s in symbols], dtype=np.int32)
@@ -184,6 +202,17 @@ class Mode:
 
     def finish(self):
         self._check(self._L.n2p2b_finish(self._h))
+
+    def set_profiling(self, enable: bool = True):
+        self._check(self._L.n2p2b_set_profiling(self._h, int(enable)))
+
+    def stage_times(self, reset: bool = True):
+        """Summed device ms per stage (NL, SF, NN, E, F) and run count."""
+        ms = (C.c_double * 5)()
+        runs = C.c_int64()
+        self._check(self._L.n2p2b_get_stage_times(self._h, ms, C.byref(runs),
+                                                  int(reset)))
+        return list(ms), runs.value
 
     def set_stream(self, stream_ptr: int | None):
         self._check(self._L.n2p2b_set_stream(

@@ -671,6 +671,14 @@ int ho_predict(ho_potential const* P, int n, double const* box,
     return 0;
 }
 
+void ho_cutoff_fdf(int type, double rc, double alpha, double r, double* fc,
+                   double* dfc)
+{
+    ho_constants();
+    ho_cutoff const c = ho_make_cutoff(type, rc, alpha);
+    ho_fdf(&c, r, fc, dfc);
+}
+
 long ho_last_num_entries(void)
 {
     long t = 0;

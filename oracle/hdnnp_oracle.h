@@ -54,6 +54,11 @@ int ho_predict(ho_potential const* P, int n, double const* box,
                double const* pos, int const* elem, double* energy,
                double* forces, double* atomic_energies);
 
+/* CutoffFunction::fdf for cutoff `type` (n2p2 numbering), radius rc and
+ * inner fraction alpha. */
+void ho_cutoff_fdf(int type, double rc, double alpha, double r, double* fc,
+                   double* dfc);
+
 /* Neighbor counts / list after the last ho_predict call's neighbor search
  * (reference order); index may be NULL to query the total only. */
 long ho_last_num_entries(void);

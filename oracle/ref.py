@@ -59,6 +59,8 @@ def _load():
     L.refh_num_slots.argtypes = [C.c_void_p, C.c_int, C.c_int]
     L.refh_max_cutoff.restype = C.c_double
     L.refh_max_cutoff.argtypes = [C.c_void_p]
+    L.refh_sf_params.restype = C.c_int
+    L.refh_sf_params.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
     L.refh_set_structure.restype = C.c_int
     L.refh_set_structure.argtypes = [C.c_void_p, C.c_int, _dp, _dp, _ip]
     L.refh_evaluate.restype = C.c_int
@@ -104,6 +106,13 @@ class RefModel:
 
     def num_slots(self, e: int, ne: int) -> int:
         return self.L.refh_num_slots(self.h, e, ne)
+
+    def sf_params(self, e: int, s: int):
+        """type, e1, e2, eta, rs, rc, zeta, lambda, scaling factor, line."""
+        out = np.zeros(10)
+        if self.L.refh_sf_params(self.h, e, s, _p(out, _dp)) != 0:
+            raise RuntimeError("unknown symmetry function type")
+        return out
 
     def set_structure(self, pos, elem, box=None):
         pos = np.ascontiguousarray(pos, dtype=np.float64).reshape(-1, 3)

@@ -19,6 +19,9 @@
 #include "Prediction.h"
 #include "Structure.h"
 #include "Atom.h"
+#include "SymFnc.h"
+#include "SymFncBaseExpAng.h"
+#include "SymFncExpRad.h"
 #include "utility.h"
 
 #include <chrono>
@@ -51,6 +54,10 @@ public:
     vector<vector<size_t>> const& sfTable(size_t e) const
     {
         return elements.at(e).getSymmetryFunctionTable();
+    }
+    SymFnc const& symmetryFunction(size_t e, size_t s) const
+    {
+        return elements.at(e).getSymmetryFunction(s);
     }
     void setupUnscaled()
     {
@@ -168,6 +175,39 @@ int refh_num_slots(void* p, int e, int ne)
 double refh_max_cutoff(void* p)
 {
     return static_cast<Handle*>(p)->model.getMaxCutoffRadius();
+}
+
+// Element::getSymmetryFunction(s) parameters: type, e1, e2 (-1 radial), eta,
+// rs, rc, zeta, lambda, scaling factor, line number.
+int refh_sf_params(void* p, int e, int s, double* out)
+{
+    Handle* h = static_cast<Handle*>(p);
+    SymFnc const& f = h->model.symmetryFunction((size_t)e, (size_t)s);
+    out[0] = (double)f.getType();
+    out[5] = f.getRc();
+    out[8] = f.getScalingFactor();
+    out[9] = (double)f.getLineNumber();
+    if (auto r = dynamic_cast<SymFncExpRad const*>(&f))
+    {
+        out[1] = (double)r->getE1();
+        out[2] = -1.0;
+        out[3] = r->getEta();
+        out[4] = r->getRs();
+        out[6] = 0.0;
+        out[7] = 0.0;
+        return 0;
+    }
+    if (auto a = dynamic_cast<SymFncBaseExpAng const*>(&f))
+    {
+        out[1] = (double)a->getE1();
+        out[2] = (double)a->getE2();
+        out[3] = a->getEta();
+        out[4] = a->getRs();
+        out[6] = a->getZeta();
+        out[7] = a->getLambda();
+        return 0;
+    }
+    return -1;
 }
 
 int refh_set_structure(void* p, int n, double const* box9, double const* pos,

@@ -1,0 +1,52 @@
+"""The C-ABI shared library loads and exports every declared entry point.
+
+No compute call is made here (this suite runs without a GPU).
+"""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from n2p2_b200 import _capi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "n2p2_b200.h")
+
+
+def declared_functions():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(n2p2b_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_entry_points():
+    names = declared_functions()
+    assert "n2p2b_evaluate" in names and "n2p2b_create" in names
+    assert len(names) >= 30
+
+
+def test_library_exports_every_declared_symbol():
+    lib = C.CDLL(_capi.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_the_header():
+    assert set(declared_functions()) <= set(_capi.SIGNATURES)
+
+
+def test_create_without_gpu_reports_cuda_error():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    L = _capi.load()
+    h = C.c_void_p()
+    assert L.n2p2b_create(0, C.byref(h)) == _capi.ERR_CUDA
+    assert not h.value
+
+
+def test_null_context_is_rejected():
+    L = _capi.load()
+    assert L.n2p2b_evaluate(None, 1) == _capi.ERR_ARGUMENT
+    assert L.n2p2b_last_error(None) == b"null context"

@@ -1,0 +1,139 @@
+"""The oracles are pinned before they are trusted.
+
+* The reference library built from the reference sources (oracle/_ref) and
+  the C restatement (oracle/hdnnp_oracle.c) both reproduce the reference's
+  own golden energies and forces of test/cpp/ExamplePrediction.h -- read from
+  the reference tree at test time, never copied -- within the reference's
+  tolerance 1000 * DBL_EPSILON (test/cpp/test_Prediction.cpp:27).
+* The restatement agrees with the reference library on the synthetic water
+  potentials (neighbor lists exactly, energies/forces to 1e-12 relative).
+"""
+import os
+
+import numpy as np
+import pytest
+
+from conftest import REFERENCE, reference_tree_available
+from oracle import ref as oref
+from oracle import restated
+
+POT = os.path.join(os.path.dirname(__file__), "golden", "potentials")
+EPS1000 = 1000.0 * np.finfo(float).eps
+EXAMPLES = ["H2O_RPBE-D3", "Cu2S_PBE"]
+
+needs_ref_tree = pytest.mark.skipif(
+    not reference_tree_available(), reason="reference tree not present")
+needs_ref_lib = pytest.mark.skipif(
+    not oref.ref_available(), reason="oracle/_ref not built")
+
+
+def _example(name):
+    d = os.path.join(REFERENCE, "examples", "nnp-predict", name)
+    fr = oref.read_input_data(os.path.join(d, "input.data"))[0]
+    syms = restated.Potential(d).symbols
+    elem = np.array([syms.index(s) for s in fr["sym"]], dtype=np.int32)
+    return d, fr, elem
+
+
+@pytest.fixture(scope="module")
+def golden():
+    return oref.read_golden_prediction(os.path.join(
+        REFERENCE, "test", "cpp", "ExamplePrediction.h"))
+
+
+@needs_ref_tree
+@needs_ref_lib
+@pytest.mark.parametrize("name", EXAMPLES)
+def test_reference_build_matches_golden(golden, name):
+    d, fr, elem = _example(name)
+    m = oref.RefModel(d)
+    m.set_structure(fr["pos"], elem, fr["box"])
+    e, f = m.predict()
+    ge, gf = golden[name]
+    assert abs(e - ge) <= EPS1000 * max(1.0, abs(ge)) or abs(e - ge) <= EPS1000
+    assert np.abs(f - gf).max() <= EPS1000
+
+
+@needs_ref_tree
+@pytest.mark.parametrize("name", EXAMPLES)
+def test_restatement_matches_golden(golden, name):
+    d, fr, elem = _example(name)
+    e, f = restated.predict(d, fr["pos"], elem, fr["box"])
+    ge, gf = golden[name]
+    assert abs(e - ge) <= EPS1000 * max(1.0, abs(ge))
+    assert np.abs(f - gf).max() <= EPS1000
+
+
+@needs_ref_lib
+@pytest.mark.parametrize("name", ["h2o_52", "h2o_92"])
+def test_restatement_matches_reference_build(name):
+    from n2p2_b200 import synth
+    d = os.path.join(POT, name)
+    box, pos, elem = synth.water_box(64, 3)
+    ref = oref.RefModel(d)
+    ref.set_structure(pos, elem, box)
+    e0, f0 = ref.predict()
+    e1, f1 = restated.predict(d, pos, elem, box)
+    assert abs(e1 - e0) <= 1e-12 * abs(e0)
+    assert np.abs(f1 - f0).max() <= 1e-12 * np.abs(f0).max()
+
+
+@needs_ref_lib
+def test_restated_neighbor_list_is_the_reference_list():
+    """Same (index, dr, d) per atom in the same order, bit for bit."""
+    from n2p2_b200 import synth
+    d = os.path.join(POT, "h2o_52")
+    box, pos, elem = synth.water_box(64, 9)
+    ref = oref.RefModel(d)
+    ref.set_structure(pos, elem, box)
+    ref.evaluate(False)
+    c0, i0, dr0, d0 = ref.neighbors()
+    restated.predict(d, pos, elem, box)
+    L = restated._load()
+    E = L.ho_last_num_entries()
+    n = len(elem)
+    cnt = np.zeros(n, dtype=np.int64)
+    idx = np.zeros(E, dtype=np.int64)
+    dr = np.zeros((E, 3))
+    dd = np.zeros(E)
+    L.ho_last_neighbors(cnt.ctypes.data, idx.ctypes.data, dr.ctypes.data,
+                        dd.ctypes.data)
+    assert np.array_equal(c0, cnt)
+    assert np.array_equal(i0, idx)
+    assert np.array_equal(dr0.view(np.int64), dr.view(np.int64))
+    assert np.array_equal(d0.view(np.int64), dd.view(np.int64))
+
+
+def cutoff_kats():
+    """(rc, alpha, r, f[9], df[9]) of test/cpp/test_CutoffFunction.cpp."""
+    import re
+    src = open(os.path.join(REFERENCE, "test", "cpp",
+                            "test_CutoffFunction.cpp")).read()
+    rc = float(re.search(r"cutoffRadius\s*=\s*([0-9.eE+-]+);", src).group(1))
+    alpha = float(re.search(r"cutoffParameter\s*=\s*([0-9.eE+-]+);",
+                            src).group(1))
+    frac = float(re.search(r"testRadius\s*=\s*([0-9.eE+-]+)\s*\*", src)
+                 .group(1))
+
+    def vec(name):
+        body = re.search(r"vector<double> const " + name + r"\s*=\s*\{(.*?)\}",
+                         src, re.S).group(1)
+        return [float(x) for x in body.replace("\n", " ").split(",")]
+    return rc, alpha, frac * rc, vec("f"), vec("df")
+
+
+@needs_ref_tree
+def test_cutoff_kats_all_types():
+    """All nine cutoff types at r = 0.8 rc (rc = 3, alpha = 0.2) against the
+    reference's known answers, tolerance 100 * DBL_EPSILON as there."""
+    import ctypes as C
+    rc, alpha, r, f, df = cutoff_kats()
+    L = restated._load()
+    L.ho_cutoff_fdf.argtypes = [C.c_int, C.c_double, C.c_double, C.c_double,
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    for t in range(9):
+        a, b = C.c_double(), C.c_double()
+        L.ho_cutoff_fdf(t, rc, alpha, r, C.byref(a), C.byref(b))
+        tol = 100 * np.finfo(float).eps
+        assert abs(a.value - f[t]) <= tol, (t, a.value, f[t])
+        assert abs(b.value - df[t]) <= tol, (t, b.value, df[t])
