@@ -183,6 +183,48 @@ int n2p2b_get_stage_times(n2p2b_context* ctx, double* ms, int64_t* runs,
 /* Number of kernel launches this library has issued in this process. */
 uint64_t n2p2b_kernel_launch_count(void);
 
+/* ---- neighbor list without memory allocation -------------------------- */
+
+/* No counterpart in the reference (n2p2 always builds neighbor lists into
+ * std::vectors it allocates).  For callers that cannot allocate device
+ * memory while they run -- an MD engine that reserves all GPU memory up
+ * front, or code that must not trigger the device-wide synchronization of
+ * cudaMalloc/cudaFree -- this computes the neighbor list of
+ * Structure::calculateNeighborList (every (j, image) with
+ * |r_i - r_j + image|^2 <= cutoff^2, bit-exact, in j-ascending, image
+ * order) into buffers the caller owns, and allocates nothing.
+ *
+ * Its only other memory is one static device array of about 1.3 MB, held by
+ * every GPU that loads this library until the process exits.  That array
+ * sets the limits: at most N2P2B_NOALLOC_MAX_ATOMS atoms and
+ * N2P2B_NOALLOC_MAX_NEIGHBORS neighbors per atom; larger inputs are
+ * rejected with N2P2B_ERR_CAPACITY and a message in `err`.  All calls share
+ * the array and it keeps the last call's contents (each call clears what
+ * must start at zero), so calls whose GPU work overlaps (other streams or
+ * host threads) race: serialize them.  The first call for a device looks up
+ * the array's device address (cudaGetSymbolAddress) and should come before
+ * any stream capture.
+ *
+ * device:    CUDA device to run on (the caller's current device is kept).
+ * stream:    cudaStream_t for the work (NULL = default stream); the call
+ *            returns after that stream has finished it.
+ * box:       host, 9 doubles (rows = lattice vectors) or NULL (non-periodic).
+ * positions: device, num_atoms x 3, used as given (no remap, no units).
+ * counts:    device, num_atoms          neighbors per atom (output)
+ * offsets:   device, num_atoms + 1      exclusive prefix of counts (output)
+ * index, dr, d: device, capacity, 3 x capacity, capacity: neighbor index,
+ *            displacement r_i - r_j + image and distance (output).
+ * total:     host, number of entries (also when capacity was too small).
+ * err:       optional host buffer for a message. */
+#define N2P2B_NOALLOC_MAX_ATOMS      65536
+#define N2P2B_NOALLOC_MAX_NEIGHBORS  1024
+int n2p2b_neighbor_list_noalloc(int device, void* stream, int64_t num_atoms,
+                                const double* box, const double* positions,
+                                double cutoff, int32_t* counts,
+                                int32_t* offsets, int32_t* index, double* dr,
+                                double* d, int64_t capacity, int64_t* total,
+                                char* err, size_t err_len);
+
 /* ---- one call per frame ----------------------------------------------- */
 
 /* Prediction::readStructureFromFile + Prediction::predict on in-memory
