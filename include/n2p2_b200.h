@@ -60,6 +60,23 @@ const char* n2p2b_last_error(const n2p2b_context* ctx);
 /* Runs the context's device work on `stream` (a cudaStream_t, NULL = own). */
 int         n2p2b_set_stream(n2p2b_context* ctx, void* stream);
 
+/* Arithmetic of the evaluation.  No counterpart in the reference (it always
+ * computes in double).  N2P2B_PRECISION_FP64 (default) is the plain form.
+ * The two mixed forms compute symmetry functions and dG/dr in FP32 and the
+ * atomic NNs on the tensor cores with BF16 operands and FP32 accumulation;
+ * neighbor displacements, the energy sum and the force accumulation stay
+ * FP64.  N2P2B_PRECISION_MIXED splits each NN operand into BF16 high and low
+ * parts (three tensor-core products per step, about 16 significant bits);
+ * N2P2B_PRECISION_BF16 uses single BF16 operands (8 significant bits).
+ * Getters return the FP32 intermediates widened to double.  Returns
+ * N2P2B_ERR_SETUP if the potential's networks do not fit the tensor-core
+ * kernel (more than one output, a layer wider than 256). */
+#define N2P2B_PRECISION_FP64     0
+#define N2P2B_PRECISION_MIXED    1
+#define N2P2B_PRECISION_BF16     2
+int         n2p2b_set_precision(n2p2b_context* ctx, int mode);
+int         n2p2b_get_precision(const n2p2b_context* ctx);
+
 /* ---- setup (nnp::Mode / nnp::Prediction) ------------------------------ */
 
 /* Mode::loadSettingsFile (libnnp/Mode.cpp:161-210). */

@@ -22,6 +22,9 @@ ERR_INTERNAL = -6
 HOST = 0
 DEVICE = 1
 REMAP = 1
+PRECISION_FP64 = 0
+PRECISION_MIXED = 1
+PRECISION_BF16 = 2
 
 _dp = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
@@ -34,6 +37,8 @@ SIGNATURES = {
     "n2p2b_destroy": (None, [_vp]),
     "n2p2b_last_error": (C.c_char_p, [_vp]),
     "n2p2b_set_stream": (C.c_int, [_vp, _vp]),
+    "n2p2b_set_precision": (C.c_int, [_vp, C.c_int]),
+    "n2p2b_get_precision": (C.c_int, [_vp]),
     "n2p2b_load_settings_file": (C.c_int, [_vp, C.c_char_p]),
     "n2p2b_setup_generic": (C.c_int, [_vp]),
     "n2p2b_setup_symmetry_function_scaling": (C.c_int, [_vp, C.c_char_p]),

@@ -187,6 +187,15 @@ struct n2p2b_context
     int          maxSF = 0;
     int          maxSlots = 0;
     DevBuf       sfScale, nnW, slotSF;
+    // Mixed forms (FP32 symmetry functions, BF16 tensor-core NNs); index 0
+    // = single BF16 operands (PREC_BF16), 1 = hi/lo split (PREC_MIXED).
+    int          precision = PREC_FP64;
+    TcNNParams   tcp[2] = {};
+    bool         tcOk[2] = {false, false};
+    std::string  tcWhy[2];
+    DevBuf       tcW[2], tcF[2];
+    int          tileBeg[kMaxElem + 1] = {};
+    int          tcGrid[2] = {0, 0};
 
     // Structure.
     long         n = 0;
@@ -285,7 +294,8 @@ struct n2p2b_context
             for (auto& e : se.ev) cudaEventDestroy(e);
         for (auto& se : freeEvents)
             for (auto& e : se.ev) cudaEventDestroy(e);
-        for (DevBuf* b : {&sfScale, &nnW, &slotSF, &posIn, &pos, &elem,
+        for (DevBuf* b : {&sfScale, &nnW, &slotSF, &tcW[0], &tcF[0], &tcW[1],
+                          &tcF[1], &posIn, &pos, &elem,
                           &atomsByElem, &cellOf, &cellCount, &cellFill,
                           &cellStart, &cellAtoms, &cellStatus, &nbrCount,
                           &nbrCountElem, &nbrOff, &keyTmp, &key, &nbrIdx,
@@ -490,6 +500,11 @@ struct n2p2b_context
         if (maxW > kMaxWidth)
             throw std::runtime_error("ERROR: NN layer wider than supported.\n");
         nnp.maxWidth = maxW;
+        std::vector<unsigned char> tcWeights[2];
+        std::vector<float> tcFloats[2];
+        for (int k = 0; k < 2; ++k)
+            tcOk[k] = tcBuild(nnp, blob, k, tcp[k], tcWeights[k], tcFloats[k],
+                              tcWhy[k]);
 
         if (hostOnly())
         {
@@ -506,6 +521,18 @@ struct n2p2b_context
         slotSF.ensure(sizeof(int16_t) * slotTab.size());
         ck(cudaMemcpy(slotSF.p, slotTab.data(), sizeof(int16_t) * slotTab.size(),
                       cudaMemcpyHostToDevice), "copy slot table");
+        for (int k = 0; k < 2; ++k)
+        {
+            tcGrid[k] = 0;
+            if (!tcOk[k]) continue;
+            tcW[k].ensure(tcWeights[k].size());
+            ck(cudaMemcpy(tcW[k].p, tcWeights[k].data(), tcWeights[k].size(),
+                          cudaMemcpyHostToDevice), "copy BF16 weights");
+            tcF[k].ensure(sizeof(float) * tcFloats[k].size());
+            ck(cudaMemcpy(tcF[k].p, tcFloats[k].data(),
+                          sizeof(float) * tcFloats[k].size(),
+                          cudaMemcpyHostToDevice), "copy FP32 NN parameters");
+        }
         tablesReady = true;
         invalidate();
     }
@@ -619,6 +646,14 @@ struct n2p2b_context
         }
         es.start[ne] = (int)byElem.size();
         for (int e = ne + 1; e <= kMaxElem; ++e) es.start[e] = es.start[ne];
+        // Tensor-core tiles: 128 atoms of one element each.
+        std::memset(tileBeg, 0, sizeof(tileBeg));
+        for (int e = 0; e < ne; ++e)
+        {
+            int const cnt = es.start[e + 1] - es.start[e];
+            tileBeg[e + 1] = tileBeg[e] + (cnt + kTcRows - 1) / kTcRows;
+        }
+        for (int e = ne + 1; e <= kMaxElem; ++e) tileBeg[e] = tileBeg[ne];
 
         posIn.ensure(sizeof(double) * 3 * n);
         pos.ensure(sizeof(double) * 3 * n);
@@ -656,9 +691,9 @@ struct n2p2b_context
         nbrCount.ensure(sizeof(int) * n);
         nbrCountElem.ensure(sizeof(int) * n * ne);
         nbrOff.ensure(sizeof(int) * (n + 1));
-        G.ensure(sizeof(double) * n * maxSF);
-        dEdG.ensure(sizeof(double) * n * maxSF);
-        dGdrSelf.ensure(sizeof(double) * n * maxSF * 3);
+        G.ensure(realBytes() * n * maxSF);
+        dEdG.ensure(realBytes() * n * maxSF);
+        dGdrSelf.ensure(realBytes() * n * maxSF * 3);
         Ei.ensure(sizeof(double) * n);
         selfF.ensure(sizeof(double) * n * 3);
         F.ensure(sizeof(double) * n * 3);
@@ -686,8 +721,55 @@ struct n2p2b_context
         entryAtom.ensure(sizeof(int) * c);
         mirror.ensure(sizeof(int) * c);
         pairF.ensure(sizeof(double) * 3 * c);
-        dGdr.ensure(sizeof(double) * 3 * (std::size_t)c
+        dGdr.ensure(realBytes() * 3 * (std::size_t)c
                     * std::max(maxSlots, 1));
+    }
+
+    // Bytes of one symmetry-function / dE/dG / dG/dr value.
+    std::size_t realBytes() const
+    {
+        return precision != PREC_FP64 ? sizeof(float) : sizeof(double);
+    }
+
+    // Copies `count` values of a per-atom real buffer to the host as double.
+    std::vector<double> readReal(DevBuf const& b, std::size_t count)
+    {
+        std::vector<double> out(count);
+        if (count == 0) return out;
+        if (precision != PREC_FP64)
+        {
+            std::vector<float> f(count);
+            ck(cudaMemcpy(f.data(), b.p, sizeof(float) * count,
+                          cudaMemcpyDeviceToHost), "read results");
+            for (std::size_t k = 0; k < count; ++k) out[k] = f[k];
+        }
+        else
+        {
+            ck(cudaMemcpy(out.data(), b.p, sizeof(double) * count,
+                          cudaMemcpyDeviceToHost), "read results");
+        }
+        return out;
+    }
+
+    void setPrecision(int mode)
+    {
+        if (mode != PREC_FP64 && mode != PREC_MIXED && mode != PREC_BF16)
+            throw std::invalid_argument("ERROR: Unknown precision mode.\n");
+        int const k = (mode == PREC_MIXED) ? 1 : 0;
+        if (mode != PREC_FP64 && tablesReady && !tcOk[k])
+            throw std::runtime_error("ERROR: The mixed-precision form cannot "
+                                     "run this potential: " + tcWhy[k]
+                                     + ".\n");
+        if (mode == precision) return;
+        precision = mode;
+        sfGrid = 0;
+        invalidate();
+        if (n > 0 && !hostOnly())
+        {
+            activate();
+            ensureStructureBuffers();
+            ensureEntryBuffers();
+        }
     }
 
     void grow(long total)
@@ -760,7 +842,7 @@ struct n2p2b_context
         {
             ck(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount,
                                       device), "device attribute");
-            sfGrid = smCount * sfBlocksPerSM(sfp, sfCap, sfVariant);
+            sfGrid = smCount * sfBlocksPerSM(sfp, sfCap, sfVariant, precision);
             sfGridCap = sfCap;
         }
         long const blocksNeeded = (n + sfAtomsPerBlock() - 1)
@@ -781,15 +863,47 @@ struct n2p2b_context
         L.dz = dz.as<double>();
         L.dd = dd.as<double>();
         L.scale = sfScale.as<SFScale>();
-        L.G = G.as<double>();
-        L.dGdrSelf = dGdrSelf.as<double>();
-        L.dGdr = dGdr.as<double>();
+        L.precision = precision;
+        L.G = G.p;
+        L.dGdrSelf = dGdrSelf.p;
+        L.dGdr = dGdr.p;
         L.status = status.as<int>();
         launchSymmetryFunctions(sfp, L, stream);
     }
 
     void enqueueNN(bool deriv)
     {
+        if (precision != PREC_FP64)
+        {
+            int const k = (precision == PREC_MIXED) ? 1 : 0;
+            if (!tcOk[k])
+                throw std::runtime_error("ERROR: The mixed-precision form "
+                                         "cannot run this potential: "
+                                         + tcWhy[k] + ".\n");
+            if (tcGrid[k] == 0)
+            {
+                ck(cudaDeviceGetAttribute(&smCount,
+                                          cudaDevAttrMultiProcessorCount,
+                                          device), "device attribute");
+                tcGrid[k] = smCount * tcBlocksPerSM(tcp[k]);
+            }
+            TcNNLaunch T;
+            T.n = (int)n;
+            T.derivatives = deriv ? 1 : 0;
+            T.maxSF = maxSF;
+            T.atomsByElem = atomsByElem.as<int>();
+            T.es = es;
+            std::memcpy(T.tileBeg, tileBeg, sizeof(tileBeg));
+            T.grid = tcGrid[k];
+            T.wblob = tcW[k].as<unsigned char>();
+            T.fblob = tcF[k].as<float>();
+            T.G = G.as<float>();
+            T.energy = Ei.as<double>();
+            T.dEdG = dEdG.as<float>();
+            T.status = status.as<int>();
+            launchNeuralNetworksTC(tcp[k], T, stream);
+            return;
+        }
         NNLaunch L;
         L.n = (int)n;
         L.derivatives = deriv ? 1 : 0;
@@ -842,9 +956,10 @@ struct n2p2b_context
             L.numSF[e] = sfp.numSF[e];
             for (int f = 0; f < ne; ++f) L.numSlots[e][f] = sfp.numSlots[e][f];
         }
-        L.dEdG = dEdG.as<double>();
-        L.dGdrSelf = dGdrSelf.as<double>();
-        L.dGdr = dGdr.as<double>();
+        L.precision = precision;
+        L.dEdG = dEdG.p;
+        L.dGdrSelf = dGdrSelf.p;
+        L.dGdr = dGdr.p;
         L.selfF = selfF.as<double>();
         L.pairF = pairF.as<double>();
         L.F = F.as<double>();
@@ -874,7 +989,7 @@ struct n2p2b_context
     {
         maxNbr = std::max(maxNbr, lastMaxNbr);
         int const cap = ((std::max(maxNbr, 1) + 8 + 15) / 16) * 16;
-        if (sfSharedBytes(sfp, cap) > 227 * 1024)
+        if (sfSharedBytes(sfp, cap, precision) > 227 * 1024)
             throw CapacityError("ERROR: An atom has more neighbors than the "
                                 "symmetry-function kernel can stage.\n");
         sfCap = std::max(cap, sfCap);
@@ -914,6 +1029,9 @@ struct n2p2b_context
             if (flags & FLAG_MIRROR_MISSING)
                 throw std::runtime_error("ERROR: Internal: neighbor list is "
                                          "not symmetric.\n");
+            if (flags & FLAG_TC_TIMEOUT)
+                throw CudaError("ERROR: A tensor-core wait of the NN kernel "
+                                "gave up; results are invalid.\n");
             if (sizing || (flags & FLAG_SF_CAPACITY))
             {
                 fitSFCap(statusHost[ST_MAX_NBR]);
@@ -975,6 +1093,9 @@ struct n2p2b_context
         if (flags & FLAG_MIRROR_MISSING)
             throw std::runtime_error("ERROR: Internal: neighbor list is not "
                                      "symmetric.\n");
+        if (flags & FLAG_TC_TIMEOUT)
+            throw CudaError("ERROR: A tensor-core wait of the NN kernel gave "
+                            "up; results are invalid.\n");
         haveNL = haveSF = haveNN = haveE = true;
         return 0;
     }
@@ -1155,6 +1276,16 @@ int n2p2b_set_stream(n2p2b_context* ctx, void* stream)
             ctx->ownStream = true;
         }
     });
+}
+
+int n2p2b_set_precision(n2p2b_context* ctx, int mode)
+{
+    return guarded(ctx, [&] { ctx->setPrecision(mode); });
+}
+
+int n2p2b_get_precision(n2p2b_context const* ctx)
+{
+    return ctx ? ctx->precision : N2P2B_ERR_ARGUMENT;
 }
 
 int n2p2b_load_settings_file(n2p2b_context* ctx, char const* path)
@@ -1446,9 +1577,8 @@ int n2p2b_get_symmetry_functions(n2p2b_context* ctx, double* G, int stride)
         if (!ctx->haveSF) throw StateError("ERROR: No symmetry functions.\n");
         if (stride < ctx->maxSF) throw std::invalid_argument("ERROR: stride");
         ctx->activate();
-        std::vector<double> g((std::size_t)ctx->n * ctx->maxSF);
-        ck(cudaMemcpy(g.data(), ctx->G.p, sizeof(double) * g.size(),
-                      cudaMemcpyDeviceToHost), "read G");
+        std::vector<double> const g =
+            ctx->readReal(ctx->G, (std::size_t)ctx->n * ctx->maxSF);
         for (long i = 0; i < ctx->n; ++i)
         {
             int const ns = ctx->sfp.numSF[ctx->elemHost[i]];
@@ -1465,9 +1595,8 @@ int n2p2b_get_dEdG(n2p2b_context* ctx, double* out, int stride)
             throw StateError("ERROR: No dE/dG.\n");
         if (stride < ctx->maxSF) throw std::invalid_argument("ERROR: stride");
         ctx->activate();
-        std::vector<double> g((std::size_t)ctx->n * ctx->maxSF);
-        ck(cudaMemcpy(g.data(), ctx->dEdG.p, sizeof(double) * g.size(),
-                      cudaMemcpyDeviceToHost), "read dEdG");
+        std::vector<double> const g =
+            ctx->readReal(ctx->dEdG, (std::size_t)ctx->n * ctx->maxSF);
         for (long i = 0; i < ctx->n; ++i)
         {
             int const ns = ctx->sfp.numSF[ctx->elemHost[i]];
@@ -1491,9 +1620,8 @@ int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sfStride,
         int const S = ctx->maxSlots;
         if (self)
         {
-            std::vector<double> g((std::size_t)n * ctx->maxSF * 3);
-            ck(cudaMemcpy(g.data(), ctx->dGdrSelf.p, sizeof(double) * g.size(),
-                          cudaMemcpyDeviceToHost), "read dGdr self");
+            std::vector<double> const g =
+                ctx->readReal(ctx->dGdrSelf, (std::size_t)n * ctx->maxSF * 3);
             for (long i = 0; i < n; ++i)
             {
                 int const ns = ctx->sfp.numSF[ctx->elemHost[i]];
@@ -1509,12 +1637,11 @@ int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sfStride,
             std::vector<long> perm;
             ctx->refOrder(off, perm);
             long const E = (long)perm.size();
-            std::vector<double> g((std::size_t)E * S * 3);
+            std::vector<double> const g =
+                ctx->readReal(ctx->dGdr, (std::size_t)E * S * 3);
             std::vector<int8_t> el(E);
             if (E > 0)
             {
-                ck(cudaMemcpy(g.data(), ctx->dGdr.p, sizeof(double) * g.size(),
-                              cudaMemcpyDeviceToHost), "read dGdr");
                 ck(cudaMemcpy(el.data(), ctx->nbrEl.p, E,
                               cudaMemcpyDeviceToHost), "read elements");
             }

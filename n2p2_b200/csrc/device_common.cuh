@@ -27,7 +27,8 @@ enum StatusFlags
     FLAG_SF_CAPACITY   = 1 << 2,  // an atom has more neighbors than the SF
                                   // kernel's shared-memory staging holds
     FLAG_MIRROR_MISSING = 1 << 3, // mirror entry not found (invariant broken)
-    FLAG_ABORT         = 1 << 4   // stop: later kernels return immediately
+    FLAG_ABORT         = 1 << 4,  // stop: later kernels return immediately
+    FLAG_TC_TIMEOUT    = 1 << 5   // a tensor-core wait gave up (bounded)
 };
 
 // Physical-unit box used by Structure::remap (before normalization).

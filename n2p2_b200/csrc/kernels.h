@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <string>
+#include <vector>
 
 #include "tables.h"
 #include "device_common.cuh"
@@ -58,15 +60,30 @@ void noteLaunches(int k);
 
 void launchNeighborList(NLLaunch const& L, cudaStream_t s);
 
-// Symmetry functions (+ derivatives), FP64.
+// Arithmetic of the per-atom stages: the plain form computes everything in
+// FP64.  The mixed forms compute symmetry functions in FP32 and the atomic
+// NNs on the tensor cores with BF16 operands and FP32 accumulation, and keep
+// FP64 for displacements, energy sums and force accumulation.  PREC_MIXED
+// splits every operand into BF16 high and low parts (three MMAs per product:
+// hi*hi + hi*lo + lo*hi, about 16 significant bits); PREC_BF16 uses the
+// high parts only (one MMA per product, 8 significant bits).
+enum Precision
+{
+    PREC_FP64 = 0,
+    PREC_MIXED = 1,
+    PREC_BF16 = 2
+};
+
+// Symmetry functions (+ derivatives).
 struct SFLaunch
 {
     int            n = 0;
     int            derivatives = 1;
+    int            precision = PREC_FP64;
     int            cap = 0;           // neighbor staging capacity per atom
     int            memberChunk = 12;  // members per register chunk
     int            grid = 0;          // persistent grid size
-    long           warpDoubles = 0;   // shared memory per warp (set by launcher)
+    long           warpBytes = 0;     // shared memory per warp (set by launcher)
     int            variant = 0;       // product-form shape / run chunking
     int            sortCats = 0;      // order work categories by partners
     int const*     elem = nullptr;
@@ -77,17 +94,17 @@ struct SFLaunch
     double const*  dz = nullptr;
     double const*  dd = nullptr;
     SFScale const* scale = nullptr;   // [element][maxSF]
-    double*        G = nullptr;       // [n][maxSF]
-    double*        dGdrSelf = nullptr;// [n][maxSF][3]
-    double*        dGdr = nullptr;    // per atom block [slot][3][neighbors]
+    // Outputs in the compute type (double, or float in the mixed form).
+    void*          G = nullptr;       // [n][maxSF]
+    void*          dGdrSelf = nullptr;// [n][maxSF][3]
+    void*          dGdr = nullptr;    // per atom block [slot][3][neighbors]
     int*           status = nullptr;
 };
 
 void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L,
                              cudaStream_t s);
-std::size_t sfSharedBytes(SFParams const& P, int cap);
-long sfWarpDoubles(SFParams const& P, int cap);
-int sfBlocksPerSM(SFParams const& P, int cap, int variant);
+std::size_t sfSharedBytes(SFParams const& P, int cap, int precision);
+int sfBlocksPerSM(SFParams const& P, int cap, int variant, int precision);
 int sfAtomsPerBlock();
 // Kernel variant matching the potential's product-form groups:
 // 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
@@ -110,6 +127,82 @@ struct NNLaunch
 void launchNeuralNetworks(NNParams const& P, NNLaunch const& L,
                           cudaStream_t s);
 
+// Atomic neural networks on the tensor cores (mixed form).  Per element the
+// hidden layers run as 128-atom x width GEMMs (tcgen05.mma, BF16 operands
+// in shared memory, FP32 accumulators in tensor memory); the single-output
+// layer is a per-atom FP32 dot product.  Widths are padded to multiples of
+// 16 with zero weights.
+constexpr int kTcMaxHidden = kMaxLayers - 2;
+constexpr int kTcRows = 128;              // atoms per tile (MMA M)
+
+struct TcLayer
+{
+    int  in, out;        // true widths
+    int  inP, outP;      // padded to multiples of 16
+    int  act;            // activation of this layer's neurons
+    int  w, wl;          // byte offsets of W (outP x inP, UMMA K-major), high
+                         // and low BF16 parts, in the element's weight region
+    int  wt, wtl;        // the same for W^T (inP x outP)
+    int  b;              // float offset of the bias (outP) in the element's
+                         // float region
+    int  fp;             // tensor-memory column of this layer's f' values
+};
+
+struct TcNet
+{
+    int     hidden;               // number of hidden layers (>= 1)
+    int     nin, ninP;            // input width (symmetry functions)
+    int     outAct;               // output-neuron activation
+    int     outW;                 // float offset of the output weights
+    int     outB;                 // float offset of the output bias
+    long    wOff;                 // byte offset of the weight region in blob
+    int     wBytes;               // bytes of the weight region (16-multiple)
+    long    fOff;                 // float offset of the float region in blob
+    int     fCount;               // floats of the float region
+    TcLayer layer[kTcMaxHidden];
+};
+
+struct TcNNParams
+{
+    int   numElements;
+    int   maxP;                   // widest padded width (A tile columns)
+    int   wMax;                   // bytes reserved for weights in smem
+    int   fMax;                   // floats reserved for the float region
+    int   split;                  // 1: hi/lo BF16 operands (3 MMAs / step)
+    int   tmemCols;               // tensor-memory columns allocated per CTA
+                                  // (accumulators, then the f' columns)
+    int   smemBytes;              // dynamic shared memory per CTA
+    TcNet net[kMaxElem];
+};
+
+struct TcNNLaunch
+{
+    int                n = 0;
+    int                derivatives = 1;
+    int                maxSF = 0;
+    int const*         atomsByElem = nullptr;
+    ElemStarts         es{};
+    int                tileBeg[kMaxElem + 1] = {};  // first tile per element
+    int                grid = 0;
+    unsigned char const* wblob = nullptr;  // BF16 weights (UMMA layout)
+    float const*       fblob = nullptr;    // FP32 biases, output weights
+    float const*       G = nullptr;        // [n][maxSF] scaled SFs
+    double*            energy = nullptr;   // [n]
+    float*             dEdG = nullptr;     // [n][maxSF]
+    int*               status = nullptr;
+};
+
+void launchNeuralNetworksTC(TcNNParams const& P, TcNNLaunch const& L,
+                            cudaStream_t s);
+// Builds the tensor-core tables and blobs from the FP64 weight blob; false
+// (with the reason) if a network does not fit the kernel.
+bool tcBuild(NNParams const& nn, std::vector<double> const& blob, int split,
+             TcNNParams& P, std::vector<unsigned char>& wblob,
+             std::vector<float>& fblob, std::string& why);
+// Resident CTAs per SM of the tensor-core NN kernel (shared and tensor
+// memory limits).
+int tcBlocksPerSM(TcNNParams const& P);
+
 // Forces (chain rule) and energy.
 struct ForceLaunch
 {
@@ -125,9 +218,10 @@ struct ForceLaunch
     int16_t const* slotSF = nullptr;  // [ec][ne][maxSlots] -> SF index
     int            numSF[kMaxElem] = {};
     int            numSlots[kMaxElem][kMaxElem] = {};
-    double const*  dEdG = nullptr;
-    double const*  dGdrSelf = nullptr;
-    double const*  dGdr = nullptr;
+    int            precision = PREC_FP64;  // type of the three inputs below
+    void const*    dEdG = nullptr;
+    void const*    dGdrSelf = nullptr;
+    void const*    dGdr = nullptr;
     double*        selfF = nullptr;   // [n][3]
     double*        pairF = nullptr;   // [entries][3]
     double*        F = nullptr;       // [n][3] output (physical units)

@@ -192,7 +192,9 @@ nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
     }
 }
 
-// Pass 1: warp per owner atom j.
+// Pass 1: warp per owner atom j.  T is the type of dE/dG and dG/dr (double,
+// or float in the mixed form); products and sums are formed in FP64.
+template <typename T>
 __global__ void __launch_bounds__(128)
 pairForceKernel(ForceLaunch const L)
 {
@@ -202,21 +204,24 @@ pairForceKernel(ForceLaunch const L)
     int const warps = blockDim.x >> 5;
     double* dE = smem + (long)w * L.maxSF;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    T const* const dEdG = static_cast<T const*>(L.dEdG);
+    T const* const dGdrSelf = static_cast<T const*>(L.dGdrSelf);
+    T const* const dGdr = static_cast<T const*>(L.dGdr);
     for (int j = blockIdx.x * warps + w; j < L.n; j += gridDim.x * warps)
     {
         int const ej = L.elem[j];
-        double const* src = L.dEdG + (long)j * L.maxSF;
-        for (int s = lane; s < L.maxSF; s += 32) dE[s] = src[s];
+        T const* src = dEdG + (long)j * L.maxSF;
+        for (int s = lane; s < L.maxSF; s += 32) dE[s] = (double)src[s];
         __syncwarp();
         // Self force.
         double fx = 0.0, fy = 0.0, fz = 0.0;
-        double const* gs = L.dGdrSelf + (long)j * L.maxSF * 3;
+        T const* gs = dGdrSelf + (long)j * L.maxSF * 3;
         int const numSF = L.numSF[ej];
         for (int s = lane; s < numSF; s += 32)
         {
-            fx -= dE[s] * gs[s * 3 + 0];
-            fy -= dE[s] * gs[s * 3 + 1];
-            fz -= dE[s] * gs[s * 3 + 2];
+            fx -= dE[s] * (double)gs[s * 3 + 0];
+            fy -= dE[s] * (double)gs[s * 3 + 1];
+            fz -= dE[s] * (double)gs[s * 3 + 2];
         }
         fx = warpSum(fx);
         fy = warpSum(fy);
@@ -230,7 +235,7 @@ pairForceKernel(ForceLaunch const L)
         // Pair terms of j's entries.
         long const b = L.nbrOff[j];
         int const cnt = L.nbrOff[j + 1] - (int)b;
-        double const* gd = L.dGdr + b * (long)L.maxSlots * 3;
+        T const* gd = dGdr + b * (long)L.maxSlots * 3;
         for (int t = lane; t < cnt; t += 32)
         {
             int const en = L.nbrEl[b + t];
@@ -241,9 +246,9 @@ pairForceKernel(ForceLaunch const L)
             for (int s = 0; s < ns; ++s)
             {
                 double const c = dE[tab[s]];
-                px -= c * gd[((long)s * 3 + 0) * cnt + t];
-                py -= c * gd[((long)s * 3 + 1) * cnt + t];
-                pz -= c * gd[((long)s * 3 + 2) * cnt + t];
+                px -= c * (double)gd[((long)s * 3 + 0) * cnt + t];
+                py -= c * (double)gd[((long)s * 3 + 1) * cnt + t];
+                pz -= c * (double)gd[((long)s * 3 + 2) * cnt + t];
             }
             L.pairF[(b + t) * 3 + 0] = px;
             L.pairF[(b + t) * 3 + 1] = py;
@@ -325,7 +330,10 @@ void launchForces(ForceLaunch const& L, cudaStream_t s)
     std::size_t const shm = sizeof(double) * warps * (std::size_t)L.maxSF;
     int const grid = (L.n + warps - 1) / warps;
     noteLaunches(2);
-    pairForceKernel<<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
+    if (L.precision != PREC_FP64)
+        pairForceKernel<float><<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
+    else
+        pairForceKernel<double><<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
     int const tb = 128;
     gatherForceKernel<<<(L.n + tb - 1) / tb > 0 ? (L.n + tb - 1) / tb : 1, tb,
                         0, s>>>(L);

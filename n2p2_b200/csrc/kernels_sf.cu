@@ -1,54 +1,61 @@
 // Host side of the symmetry-function stage: shared-memory sizing, occupancy
-// and dispatch to the kernel instantiated for the potential's cutoff type
-// (kernels_sf_{cos,tanhu,poly2,any}.cu, templates in sf_impl.cuh).
+// and dispatch to the kernel instantiated for the potential's cutoff type and
+// the context's precision (kernels_sf_{cos,tanhu,poly2,any}{,_f32}.cu,
+// templates in sf_impl.cuh).
 #include "kernels.h"
 #include "sf_impl.cuh"
 
 namespace n2p2b
 {
 
-void sfLaunch_1(SFParams const&, SFLaunch const&, std::size_t, cudaStream_t,
-                int);
-void sfLaunch_2(SFParams const&, SFLaunch const&, std::size_t, cudaStream_t,
-                int);
-void sfLaunch_6(SFParams const&, SFLaunch const&, std::size_t, cudaStream_t,
-                int);
-void sfLaunch_any(SFParams const&, SFLaunch const&, std::size_t, cudaStream_t,
-                  int);
-int sfBlocks_1(std::size_t, int);
-int sfBlocks_2(std::size_t, int);
-int sfBlocks_6(std::size_t, int);
-int sfBlocks_any(std::size_t, int);
+#define N2P2B_SF_DECL(SUFFIX)                                                 \
+    void sfLaunch_##SUFFIX(SFParams const&, SFLaunch const&, std::size_t,     \
+                           cudaStream_t, int);                                \
+    int sfBlocks_##SUFFIX(std::size_t, int);
+N2P2B_SF_DECL(1)
+N2P2B_SF_DECL(2)
+N2P2B_SF_DECL(6)
+N2P2B_SF_DECL(any)
+N2P2B_SF_DECL(1f)
+N2P2B_SF_DECL(2f)
+N2P2B_SF_DECL(6f)
+N2P2B_SF_DECL(anyf)
+#undef N2P2B_SF_DECL
 
-long sfWarpDoubles(SFParams const& P, int cap)
+namespace
 {
-    long const words = (cap + 31) / 32;
-    long d = 7L * cap + (long)P.maxExp * cap + 4L * P.maxSF;
-    d += (cap * words + 1) / 2;  // validity bits (uint32) in double units
-    d += (long)(sfk::kMaxCats * sizeof(sfk::Cat) + 7) / 8;  // categories
-    return d + 1;
+
+long warpBytesFor(SFParams const& P, int cap, int precision)
+{
+    return precision != PREC_FP64
+        ? sfk::warpBytes<float>(P.maxExp, P.maxSF, cap)
+        : sfk::warpBytes<double>(P.maxExp, P.maxSF, cap);
 }
 
-std::size_t sfSharedBytes(SFParams const& P, int cap)
+} // namespace
+
+std::size_t sfSharedBytes(SFParams const& P, int cap, int precision)
 {
     int const ng = P.groupBeg[P.numElements];
     int nm = 0;
     if (ng > 0) nm = P.groups[ng - 1].mbeg + P.groups[ng - 1].mcnt;
     return sfk::tableBytes(ng, nm)
-         + sizeof(double) * sfk::kWarps * sfWarpDoubles(P, cap);
+         + (std::size_t)sfk::kWarps * warpBytesFor(P, cap, precision);
 }
 
 int sfAtomsPerBlock() { return sfk::kWarps; }
 
-int sfBlocksPerSM(SFParams const& P, int cap, int variant)
+int sfBlocksPerSM(SFParams const& P, int cap, int variant, int precision)
 {
-    std::size_t const shm = sfSharedBytes(P, cap);
+    std::size_t const shm = sfSharedBytes(P, cap, precision);
+    bool const f = precision != PREC_FP64;
     switch (P.cutoffType)
     {
-    case 1: return sfBlocks_1(shm, variant);
-    case 2: return sfBlocks_2(shm, variant);
-    case 6: return sfBlocks_6(shm, variant);
-    default: return sfBlocks_any(shm, variant);
+    case 1: return f ? sfBlocks_1f(shm, variant) : sfBlocks_1(shm, variant);
+    case 2: return f ? sfBlocks_2f(shm, variant) : sfBlocks_2(shm, variant);
+    case 6: return f ? sfBlocks_6f(shm, variant) : sfBlocks_6(shm, variant);
+    default:
+        return f ? sfBlocks_anyf(shm, variant) : sfBlocks_any(shm, variant);
     }
 }
 
@@ -68,15 +75,22 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,
                              cudaStream_t s)
 {
     SFLaunch L = L0;
-    L.warpDoubles = sfWarpDoubles(P, L.cap);
-    std::size_t const shm = sfSharedBytes(P, L.cap);
+    L.warpBytes = warpBytesFor(P, L.cap, L.precision);
+    std::size_t const shm = sfSharedBytes(P, L.cap, L.precision);
     noteLaunches(1);
+    bool const f = L.precision != PREC_FP64;
+    int const v = L.variant;
     switch (P.cutoffType)
     {
-    case 1: sfLaunch_1(P, L, shm, s, L.variant); break;
-    case 2: sfLaunch_2(P, L, shm, s, L.variant); break;
-    case 6: sfLaunch_6(P, L, shm, s, L.variant); break;
-    default: sfLaunch_any(P, L, shm, s, L.variant); break;
+    case 1: f ? sfLaunch_1f(P, L, shm, s, v) : sfLaunch_1(P, L, shm, s, v);
+            break;
+    case 2: f ? sfLaunch_2f(P, L, shm, s, v) : sfLaunch_2(P, L, shm, s, v);
+            break;
+    case 6: f ? sfLaunch_6f(P, L, shm, s, v) : sfLaunch_6(P, L, shm, s, v);
+            break;
+    default: f ? sfLaunch_anyf(P, L, shm, s, v)
+               : sfLaunch_any(P, L, shm, s, v);
+            break;
     }
 }
 

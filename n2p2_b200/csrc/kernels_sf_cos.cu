@@ -1,19 +1,20 @@
-// Symmetry-function kernels instantiated for cutoff type 1.
-// One translation unit per cutoff type so the variants compile in parallel.
+// Symmetry-function kernels instantiated for cutoff type 1, FP64 (plain form).
+// One translation unit per (cutoff type, precision) so the variants compile
+// in parallel.
 #include "sf_impl.cuh"
 
 namespace n2p2b
 {
 
 void sfLaunch_1(SFParams const& P, SFLaunch const& L, std::size_t shm,
-                  cudaStream_t s, int variant)
+                   cudaStream_t s, int variant)
 {
-    sfk::launchForCT<1>(P, L, shm, s, variant);
+    sfk::launchForCT<double, 1>(P, L, shm, s, variant);
 }
 
 int sfBlocks_1(std::size_t shm, int variant)
 {
-    return sfk::blocksForCT<1>(shm, variant);
+    return sfk::blocksForCT<double, 1>(shm, variant);
 }
 
 } // namespace n2p2b

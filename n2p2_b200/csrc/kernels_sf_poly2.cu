@@ -1,19 +1,20 @@
-// Symmetry-function kernels instantiated for cutoff type 6.
-// One translation unit per cutoff type so the variants compile in parallel.
+// Symmetry-function kernels instantiated for cutoff type 6, FP64 (plain form).
+// One translation unit per (cutoff type, precision) so the variants compile
+// in parallel.
 #include "sf_impl.cuh"
 
 namespace n2p2b
 {
 
 void sfLaunch_6(SFParams const& P, SFLaunch const& L, std::size_t shm,
-                  cudaStream_t s, int variant)
+                   cudaStream_t s, int variant)
 {
-    sfk::launchForCT<6>(P, L, shm, s, variant);
+    sfk::launchForCT<double, 6>(P, L, shm, s, variant);
 }
 
 int sfBlocks_6(std::size_t shm, int variant)
 {
-    return sfk::blocksForCT<6>(shm, variant);
+    return sfk::blocksForCT<double, 6>(shm, variant);
 }
 
 } // namespace n2p2b

@@ -1,5 +1,7 @@
-// Symmetry functions and their derivatives, FP64 (plain form) -- kernel
-// templates, instantiated per cutoff type by kernels_sf_ct*.cu.
+// Symmetry functions and their derivatives -- kernel templates, instantiated
+// per cutoff type and compute type by kernels_sf_*.cu.  R = double is the
+// plain form; R = float is the precision form (neighbor displacements are
+// FP64 in memory and rounded to FP32 when staged; outputs are FP32).
 //
 // Semantics: Element::calculateSymmetryFunctionGroups driving
 //   SymGrpExpRad::calculate   (libnnp/SymGrpExpRad.cpp:144-239)   type 2
@@ -39,7 +41,7 @@
 //   p3   = fn * vexp_eta * A_s * (zl_s X3 + plambda_s (2 eta pfc - pr3))
 // with X1 = pfc (1/(r_ij r_ik) - cos/r_ij^2), X3 = pfc/(r_ij r_ik), zl = zeta
 // lambda and fn the member's 2^(1-zeta) * scaling factor.  Per pair one exp
-// per eta run and one power per shape remain; each member costs 9 FP64
+// per eta run and one power per shape remain; each member costs 9
 // operations.  Other groups take the general path, which keeps the
 // reference's expression form.
 //
@@ -70,128 +72,150 @@ constexpr int kThreads = 32 * kWarps;
 constexpr int kGenericChunk = 6;
 constexpr unsigned kFull = 0xffffffffu;
 
+// Math in the compute type.
+__device__ __forceinline__ double mexp(double x) { return exp(x); }
+__device__ __forceinline__ float mexp(float x) { return expf(x); }
+__device__ __forceinline__ double mtanh(double x) { return tanh(x); }
+__device__ __forceinline__ float mtanh(float x) { return tanhf(x); }
+__device__ __forceinline__ double mpow(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float mpow(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ double mrsqrt(double x) { return rsqrt(x); }
+__device__ __forceinline__ float mrsqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ void msincospi(double x, double* s, double* c)
+{
+    sincospi(x, s, c);
+}
+__device__ __forceinline__ void msincospi(float x, float* s, float* c)
+{
+    sincospif(x, s, c);
+}
+
 // CutoffFunction::fdf specialized on the (global) cutoff type; CT = -1
 // dispatches at run time.
-template <int CT>
+template <typename R, int CT>
 __device__ __forceinline__ void cutoffFdf(SFParams const& P, DevGroup const& g,
-                                          double r, double& fc, double& dfc);
+                                          R r, R& fc, R& dfc);
 
-template <int CT>
+template <typename R, int CT>
 __device__ __forceinline__ void cutoffFdfT(SFParams const& P, DevGroup const& g,
-                                           double r, double& fc, double& dfc)
+                                           R r, R& fc, R& dfc)
 {
-    if (r >= g.rc)
+    R const rcinv = R(g.rcinv);
+    R const iw = R(g.iw);
+    if (r >= R(g.rc))
     {
-        fc = 0.0;
-        dfc = 0.0;
+        fc = R(0);
+        dfc = R(0);
         return;
     }
     if (CT == 0)
     {
-        fc = 1.0;
-        dfc = 0.0;
+        fc = R(1);
+        dfc = R(0);
     }
     else if (CT == 2 || CT == 3)   // CT_TANHU, CT_TANH
     {
-        double const temp = tanh(1.0 - r * g.rcinv);
-        double const temp2 = temp * temp;
-        double const pre = (CT == 3) ? P.TANH_PRE : 1.0;
+        R const temp = mtanh(R(1) - r * rcinv);
+        R const temp2 = temp * temp;
+        R const pre = (CT == 3) ? R(P.TANH_PRE) : R(1);
         fc = pre * temp * temp2;
-        dfc = 3.0 * pre * temp2 * (temp2 - 1.0) * g.rcinv;
+        dfc = R(3) * pre * temp2 * (temp2 - R(1)) * rcinv;
     }
     else
     {
-        if (r < g.rci)
+        if (r < R(g.rci))
         {
-            fc = 1.0;
-            dfc = 0.0;
+            fc = R(1);
+            dfc = R(0);
             return;
         }
-        double const x = (r - g.rci) * g.iw;
+        R const x = (r - R(g.rci)) * iw;
         if (CT == 1)               // CT_COS: d/dr cos uses sin(pi x) >= 0
         {
-            double s, c;
-            sincospi(x, &s, &c);
-            fc = 0.5 * (c + 1.0);
-            dfc = -0.5 * g.iw * P.PI * s;
+            R s, c;
+            msincospi(x, &s, &c);
+            fc = R(0.5) * (c + R(1));
+            dfc = R(-0.5) * iw * R(P.PI) * s;
         }
         else
         {
-            double fx, dfx;
+            R fx, dfx;
             if (CT == 4)           // CT_EXP
             {
-                double const temp = 1.0 / (x * x - 1.0);
-                double const temp2 = exp(temp);
-                fx = P.E * temp2;
-                dfx = -2.0 * P.E * x * temp * temp * temp2;
+                R const temp = R(1) / (x * x - R(1));
+                R const temp2 = mexp(temp);
+                fx = R(P.E) * temp2;
+                dfx = R(-2) * R(P.E) * x * temp * temp * temp2;
             }
             else if (CT == 5)      // CT_POLY1
             {
-                fx = (2.0 * x - 3.0) * x * x + 1.0;
-                dfx = x * (6.0 * x - 6.0);
+                fx = (R(2) * x - R(3)) * x * x + R(1);
+                dfx = x * (R(6) * x - R(6));
             }
             else if (CT == 6)      // CT_POLY2
             {
-                double const x2 = x * x;
-                fx = ((15.0 - 6.0 * x) * x - 10.0) * x * x2 + 1.0;
-                dfx = x2 * ((60.0 - 30.0 * x) * x - 30.0);
+                R const x2 = x * x;
+                fx = ((R(15) - R(6) * x) * x - R(10)) * x * x2 + R(1);
+                dfx = x2 * ((R(60) - R(30) * x) * x - R(30));
             }
             else if (CT == 7)      // CT_POLY3
             {
-                double const x2 = x * x;
-                fx = (x * (x * (20.0 * x - 70.0) + 84.0) - 35.0) * x2 * x2
-                     + 1.0;
-                dfx = x2 * x * (x * (x * (140.0 * x - 420.0) + 420.0) - 140.0);
+                R const x2 = x * x;
+                fx = (x * (x * (R(20) * x - R(70)) + R(84)) - R(35)) * x2 * x2
+                     + R(1);
+                dfx = x2 * x * (x * (x * (R(140) * x - R(420)) + R(420))
+                                - R(140));
             }
             else                   // CT_POLY4
             {
-                double x4 = x * x;
+                R x4 = x * x;
                 x4 *= x4;
-                fx = (x * (x * ((315.0 - 70.0 * x) * x - 540.0) + 420.0)
-                      - 126.0) * x * x4 + 1.0;
-                dfx = x4 * (x * (x * ((2520.0 - 630.0 * x) * x - 3780.0)
-                                 + 2520.0) - 630.0);
+                fx = (x * (x * ((R(315) - R(70) * x) * x - R(540)) + R(420))
+                      - R(126)) * x * x4 + R(1);
+                dfx = x4 * (x * (x * ((R(2520) - R(630) * x) * x - R(3780))
+                                 + R(2520)) - R(630));
             }
             fc = fx;
-            dfc = dfx * g.iw;
+            dfc = dfx * iw;
         }
     }
 }
 
-template <int CT>
+template <typename R, int CT>
 __device__ __forceinline__ void cutoffFdf(SFParams const& P, DevGroup const& g,
-                                          double r, double& fc, double& dfc)
+                                          R r, R& fc, R& dfc)
 {
     if (CT >= 0)
     {
-        cutoffFdfT<(CT >= 0 ? CT : 0)>(P, g, r, fc, dfc);
+        cutoffFdfT<R, (CT >= 0 ? CT : 0)>(P, g, r, fc, dfc);
         return;
     }
     switch (P.cutoffType)
     {
-    case 0: cutoffFdfT<0>(P, g, r, fc, dfc); break;
-    case 1: cutoffFdfT<1>(P, g, r, fc, dfc); break;
-    case 2: cutoffFdfT<2>(P, g, r, fc, dfc); break;
-    case 3: cutoffFdfT<3>(P, g, r, fc, dfc); break;
-    case 4: cutoffFdfT<4>(P, g, r, fc, dfc); break;
-    case 5: cutoffFdfT<5>(P, g, r, fc, dfc); break;
-    case 6: cutoffFdfT<6>(P, g, r, fc, dfc); break;
-    case 7: cutoffFdfT<7>(P, g, r, fc, dfc); break;
-    default: cutoffFdfT<8>(P, g, r, fc, dfc); break;
+    case 0: cutoffFdfT<R, 0>(P, g, r, fc, dfc); break;
+    case 1: cutoffFdfT<R, 1>(P, g, r, fc, dfc); break;
+    case 2: cutoffFdfT<R, 2>(P, g, r, fc, dfc); break;
+    case 3: cutoffFdfT<R, 3>(P, g, r, fc, dfc); break;
+    case 4: cutoffFdfT<R, 4>(P, g, r, fc, dfc); break;
+    case 5: cutoffFdfT<R, 5>(P, g, r, fc, dfc); break;
+    case 6: cutoffFdfT<R, 6>(P, g, r, fc, dfc); break;
+    case 7: cutoffFdfT<R, 7>(P, g, r, fc, dfc); break;
+    default: cutoffFdfT<R, 8>(P, g, r, fc, dfc); break;
     }
 }
 
 // pow_int (libnnp/utility.cpp:292-317): exponentiation by squaring.
-__device__ __forceinline__ double powInt(double x, int n)
+template <typename R>
+__device__ __forceinline__ R powInt(R x, int n)
 {
     unsigned m;
     if (n < 0)
     {
-        x = 1.0 / x;
+        x = R(1) / x;
         m = (unsigned)(-n);
     }
     else m = (unsigned)n;
-    double result = 1.0;
+    R result = R(1);
     do
     {
         if (m & 1u) result *= x;
@@ -202,27 +226,21 @@ __device__ __forceinline__ double powInt(double x, int n)
     return result;
 }
 
-__device__ __forceinline__ double wsum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-    return v;
-}
-
 // Per-warp shared-memory views.
+template <typename R>
 struct WarpMem
 {
-    double*   dx;
-    double*   dy;
-    double*   dz;
-    double*   d;
-    double*   inv;    // 1 / d
-    double*   fc;
-    double*   dfcr;   // dfc / d
-    double*   E;      // [expIdx][cap]
+    R*        dx;
+    R*        dy;
+    R*        dz;
+    R*        d;
+    R*        inv;    // 1 / d
+    R*        fc;
+    R*        dfcr;   // dfc / d
+    R*        E;      // [expIdx][cap]
     unsigned* bits;   // [owner][words]
-    double*   wpG;    // [maxSF]
-    double*   wpS;    // [maxSF][3]
+    R*        wpG;    // [maxSF]
+    R*        wpS;    // [maxSF][3]
     struct Cat*  cats;  // work-item categories of the current segment
     int          sortCats;  // order angular categories by partner count
 };
@@ -238,24 +256,37 @@ struct Cat
 constexpr int kMaxSegGroups = 16;
 constexpr int kMaxCats = 2 * kMaxSegGroups;
 
+// Bytes of one warp's shared-memory region (16-byte multiple).
+template <typename R>
+__host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap)
+{
+    long const words = (cap + 31) / 32;
+    long b = (long)sizeof(R) * (7L * cap + (long)maxExp * cap + 4L * maxSF);
+    b = (b + 15) / 16 * 16;
+    b += 4L * cap * words;                          // validity bits
+    b = (b + 15) / 16 * 16;
+    b += (long)(kMaxCats * sizeof(Cat));            // categories
+    return (b + 15) / 16 * 16;
+}
+
 // Adds each lane's (G, self) contribution for symmetry function `sf` (-1 =
 // nothing) into the warp sums.  `key` identifies the lane's work-item
 // category; lanes of one category occupy contiguous lanes (items are
 // enumerated category by category).  One segmented butterfly reduces every
 // run at once in a fixed lane order; the runs' first lanes then add their
 // totals one after another (two runs may share sf).
-__device__ __forceinline__ void flushBySF(WarpMem const& W, int key, int sf,
-                                          double g, double sx, double sy,
-                                          double sz)
+template <typename R>
+__device__ __forceinline__ void flushBySF(WarpMem<R> const& W, int key, int sf,
+                                          R g, R sx, R sy, R sz)
 {
     int const lane = threadIdx.x & 31;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1)
     {
-        double const a = __shfl_down_sync(kFull, g, off);
-        double const b = __shfl_down_sync(kFull, sx, off);
-        double const c = __shfl_down_sync(kFull, sy, off);
-        double const e = __shfl_down_sync(kFull, sz, off);
+        R const a = __shfl_down_sync(kFull, g, off);
+        R const b = __shfl_down_sync(kFull, sx, off);
+        R const c = __shfl_down_sync(kFull, sy, off);
+        R const e = __shfl_down_sync(kFull, sz, off);
         int const ko = __shfl_down_sync(kFull, key, off);
         if (lane + off < 32 && ko == key)
         {
@@ -295,9 +326,10 @@ struct Item
 // returns the number of items.  Angular categories are ordered by partner
 // count, largest first (stable), so that the lanes of a round have similar
 // trip counts.
+template <typename R>
 __device__ __forceinline__ int buildCats(DevGroup const* G, int g0, int g1,
                                          int const eb[kMaxElem + 1],
-                                         bool byPartners, WarpMem const& W,
+                                         bool byPartners, WarpMem<R> const& W,
                                          int& ncat)
 {
     int const lane = threadIdx.x & 31;
@@ -340,7 +372,8 @@ __device__ __forceinline__ int buildCats(DevGroup const* G, int g0, int g1,
     return total;
 }
 
-__device__ __forceinline__ Item itemOf(WarpMem const& W, int ncat, int q)
+template <typename R>
+__device__ __forceinline__ Item itemOf(WarpMem<R> const& W, int ncat, int q)
 {
     Item it;
     it.gi = -1;
@@ -379,10 +412,10 @@ __device__ __forceinline__ unsigned rangeMask(unsigned m, int w, int pb, int pe)
     return m;
 }
 
-template <int MC>
+template <typename R, int MC>
 __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
                               int g1, int const eb[kMaxElem + 1], int cnt,
-                              WarpMem const& W, double* __restrict__ out,
+                              WarpMem<R> const& W, R* __restrict__ out,
                               int derivatives)
 {
     int const lane = threadIdx.x & 31;
@@ -396,10 +429,10 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
         bool const active = it.gi >= 0;
         DevGroup const& g = G[active ? it.gi : g0];
         int const t = it.t;
-        double const r = W.d[t];
-        bool const valid = active && (r < g.rc);
-        double const pfc = W.fc[t], pdfcr = W.dfcr[t], inv = W.inv[t];
-        double const d1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        R const r = W.d[t];
+        bool const valid = active && (r < R(g.rc));
+        R const pfc = W.fc[t], pdfcr = W.dfcr[t], inv = W.inv[t];
+        R const d1[3] = {W.dx[t], W.dy[t], W.dz[t]};
         for (int mb = 0; mb < maxM; mb += MC)
         {
 #pragma unroll
@@ -407,18 +440,19 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
             {
                 bool const has = active && (mb + l < g.mcnt);
                 DevMember const& m = M[g.mbeg + (has ? mb + l : 0)];
-                double gs = 0.0, p1 = 0.0;
+                R gs = R(0), p1 = R(0);
                 if (has && valid)
                 {
                     // SymGrpExpRad.cpp:210-211 with (f_c' - 2 eta (r - rs) f_c)/r
                     // written as f_c'/r - 2 eta (r - rs) f_c / r.
-                    double const rr = r - m.rs;
-                    double const pexp = exp(-m.eta * rr * rr);
+                    R const eta = R(m.eta);
+                    R const rr = r - R(m.rs);
+                    R const pexp = mexp(-eta * rr * rr);
                     gs = pexp * pfc;
-                    p1 = m.factorNorm * (pdfcr - 2.0 * m.eta * rr * pfc * inv)
-                       * pexp;
+                    p1 = R(m.factorNorm)
+                       * (pdfcr - R(2) * eta * rr * pfc * inv) * pexp;
                 }
-                double const sx = p1 * d1[0], sy = p1 * d1[1], sz = p1 * d1[2];
+                R const sx = p1 * d1[0], sy = p1 * d1[1], sz = p1 * d1[2];
                 if (derivatives && has)
                 {
                     long const s = m.slot[it.et];
@@ -433,12 +467,12 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
 }
 
 // General angular path: the reference's per-member expression form.
-template <int CT, int MC, bool NARROW>
+template <typename R, int CT, int MC, bool NARROW>
 __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                                DevMember const* M, int g0, int g1,
                                int const eb[kMaxElem + 1], int cnt, int words,
-                               int capE, WarpMem const& W,
-                               double* __restrict__ out, int derivatives)
+                               int capE, WarpMem<R> const& W,
+                               R* __restrict__ out, int derivatives)
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
@@ -451,29 +485,29 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
         bool const active = it.gi >= 0;
         DevGroup const& g = G[active ? it.gi : g0];
         int const t = it.t;
-        double const rij = W.d[t];
-        bool const valid = active && (rij < g.rc);
-        double const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
-        double const invij = W.inv[t];
-        double const pfcij = W.fc[t];
-        double const pdfcrij = W.dfcr[t];
-        double const rc = g.rc;
+        R const rij = W.d[t];
+        R const rc = R(g.rc);
+        bool const valid = active && (rij < rc);
+        R const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        R const invij = W.inv[t];
+        R const pfcij = W.fc[t];
+        R const pdfcrij = W.dfcr[t];
         for (int mb = 0; mb < maxM; mb += MC)
         {
             int const mc = active ? min(MC, g.mcnt - mb) : 0;
-            double aG[MC], aP1[MC], aPx[MC], aPy[MC], aPz[MC];
+            R aG[MC], aP1[MC], aPx[MC], aPy[MC], aPz[MC];
 #pragma unroll
             for (int l = 0; l < MC; ++l)
             {
-                aG[l] = 0.0;
-                aP1[l] = 0.0;
-                aPx[l] = 0.0;
-                aPy[l] = 0.0;
-                aPz[l] = 0.0;
+                aG[l] = R(0);
+                aP1[l] = R(0);
+                aPx[l] = R(0);
+                aPy[l] = R(0);
+                aPz[l] = R(0);
             }
             if (valid && mc > 0)
             {
-                double const cr0 = invij * invij;  // 1 / r_ij^2
+                R const cr0 = invij * invij;  // 1 / r_ij^2
                 int const wb = it.pb >> 5;
                 int const we = (it.pe + 31) >> 5;
                 for (int w = wb; w < we; ++w)
@@ -488,26 +522,26 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                         {
                             if (k == t || !(W.d[k] < rc)) continue;
                         }
-                        double const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
-                        double const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1],
-                                               dr2[2] - dr1[2]};
-                        double const invik = W.inv[k];
-                        double const pfcik = W.fc[k];
-                        double const rinvijik = invij * invik;
-                        double const costijk = (dr1[0] * dr2[0] + dr1[1] * dr2[1]
-                                                + dr1[2] * dr2[2]) * rinvijik;
-                        double const cr = costijk * cr0;
-                        double rjk = 0.0, invjk = 0.0, pfcjk = 1.0,
-                               pdfcjk = 0.0;
+                        R const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
+                        R const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1],
+                                          dr2[2] - dr1[2]};
+                        R const invik = W.inv[k];
+                        R const pfcik = W.fc[k];
+                        R const rinvijik = invij * invik;
+                        R const costijk = (dr1[0] * dr2[0] + dr1[1] * dr2[1]
+                                           + dr1[2] * dr2[2]) * rinvijik;
+                        R const cr = costijk * cr0;
+                        R rjk = R(0), invjk = R(0), pfcjk = R(1),
+                          pdfcjk = R(0);
                         if (NARROW)
                         {
-                            double const r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1]
-                                            + dr3[2] * dr3[2];
-                            invjk = rsqrt(r2);
+                            R const r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1]
+                                       + dr3[2] * dr3[2];
+                            invjk = mrsqrt(r2);
                             rjk = r2 * invjk;
-                            cutoffFdf<CT>(P, g, rjk, pfcjk, pdfcjk);
+                            cutoffFdf<R, CT>(P, g, rjk, pfcjk, pdfcjk);
                         }
-                        double pfc, pr1, pr3 = 0.0;
+                        R pfc, pr1, pr3 = R(0);
                         if (NARROW)
                         {
                             pfc = pfcij * pfcik * pfcjk;
@@ -519,7 +553,7 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                             pfc = pfcij * pfcik;
                             pr1 = pfcik * pdfcrij;
                         }
-                        double vexp = 0.0;
+                        R vexp = R(0);
 #pragma unroll
                         for (int l = 0; l < MC; ++l)
                         {
@@ -527,35 +561,35 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                             DevMember const& mm = M[g.mbeg + mb + l];
                             if (mm.calcExp || l == 0)
                             {
-                                double const* E = W.E + (long)mm.expIdx * capE;
+                                R const* E = W.E + (long)mm.expIdx * capE;
                                 vexp = E[t] * E[k];
                                 if (NARROW)
                                 {
-                                    double const rjks = rjk - mm.rs;
-                                    vexp *= exp(-mm.eta * rjks * rjks);
+                                    R const rjks = rjk - R(mm.rs);
+                                    vexp *= mexp(-R(mm.eta) * rjks * rjks);
                                 }
                             }
-                            double const plambda = 1.0 + mm.lambda * costijk;
-                            double fg = vexp;
-                            if (plambda <= 0.0) fg = 0.0;
+                            R const plambda = R(1) + R(mm.lambda) * costijk;
+                            R fg = vexp;
+                            if (plambda <= R(0)) fg = R(0);
                             else if (mm.useIntPow)
                                 fg *= powInt(plambda, mm.zetaInt - 1);
                             else
-                                fg *= pow(plambda, mm.zeta - 1.0);
+                                fg *= mpow(plambda, R(mm.zeta) - R(1));
                             aG[l] += fg * plambda * pfc;
-                            fg *= mm.factorNorm;
-                            double const pfczl = pfc * mm.zetaLambda;
-                            double const p2etapl = plambda * mm.factorDeriv;
-                            double p1, p3;
+                            fg *= R(mm.factorNorm);
+                            R const pfczl = pfc * R(mm.zetaLambda);
+                            R const p2etapl = plambda * R(mm.factorDeriv);
+                            R p1, p3;
                             if (mm.rsPositive)
                             {
-                                double const rijs = rij - mm.rs;
+                                R const rijs = rij - R(mm.rs);
                                 p1 = fg * (pfczl * (rinvijik - cr
                                                     - p2etapl * rijs * invij)
                                            + pr1 * plambda);
                                 if (NARROW)
                                 {
-                                    double const rjks = rjk - mm.rs;
+                                    R const rjks = rjk - R(mm.rs);
                                     p3 = fg * (pfczl * (rinvijik
                                                         + p2etapl * rjks * invjk)
                                                - pr3 * plambda);
@@ -584,9 +618,9 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
             {
                 bool const has = l < mc;
                 DevMember const& mm = M[g.mbeg + (has ? mb + l : 0)];
-                double const sx = aP1[l] * dr1[0];
-                double const sy = aP1[l] * dr1[1];
-                double const sz = aP1[l] * dr1[2];
+                R const sx = aP1[l] * dr1[0];
+                R const sy = aP1[l] * dr1[1];
+                R const sz = aP1[l] * dr1[2];
                 if (derivatives && has)
                 {
                     long const s = mm.slot[it.et];
@@ -594,8 +628,8 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                     out[(s * 3 + 1) * cnt + t] = -(sy + aPy[l]);
                     out[(s * 3 + 2) * cnt + t] = -(sz + aPz[l]);
                 }
-                flushBySF(W, it.key, has ? (int)mm.sf : -1, 0.5 * aG[l], sx,
-                          sy, sz);
+                flushBySF(W, it.key, has ? (int)mm.sf : -1, R(0.5) * aG[l],
+                          sx, sy, sz);
             }
         }
     }
@@ -603,12 +637,12 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
 
 // Product-form angular path (see the header comment): NS shapes per eta
 // run, NRC runs per register chunk.
-template <int CT, int NS, int NRC, bool NARROW>
+template <typename R, int CT, int NS, int NRC, bool NARROW>
 __device__ void angularFast(SFParams const& P, DevGroup const* G,
                             DevMember const* M, int g0, int g1,
                             int const eb[kMaxElem + 1], int cnt, int words,
-                            int capE, WarpMem const& W,
-                            double* __restrict__ out, int derivatives)
+                            int capE, WarpMem<R> const& W,
+                            R* __restrict__ out, int derivatives)
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
@@ -622,53 +656,53 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
         DevGroup const& g = G[active ? it.gi : g0];
         int const t = it.t;
         int const nr = active ? g.mcnt / NS : 0;
-        double const rij = W.d[t];
-        bool const valid = active && (rij < g.rc);
-        double const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
-        double const invij = W.inv[t];
-        double const pfcij = W.fc[t];
-        double const pdfcrij = W.dfcr[t];
-        double const rc = g.rc;
+        R const rij = W.d[t];
+        R const rc = R(g.rc);
+        bool const valid = active && (rij < rc);
+        R const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        R const invij = W.inv[t];
+        R const pfcij = W.fc[t];
+        R const pdfcrij = W.dfcr[t];
         // Shape parameters (identical for every run of the group).
-        double lam[NS], zl[NS];
+        R lam[NS], zl[NS];
         int zi[NS];
 #pragma unroll
         for (int s = 0; s < NS; ++s)
         {
             DevMember const& mm = M[g.mbeg + s];
-            lam[s] = mm.lambda;
-            zl[s] = mm.zetaLambda;
+            lam[s] = R(mm.lambda);
+            zl[s] = R(mm.zetaLambda);
             zi[s] = mm.zetaInt;
         }
         for (int rb = 0; rb < maxR; rb += NRC)
         {
-            double aG[NRC][NS], aP1[NRC][NS], aPx[NRC][NS], aPy[NRC][NS],
-                   aPz[NRC][NS];
+            R aG[NRC][NS], aP1[NRC][NS], aPx[NRC][NS], aPy[NRC][NS],
+              aPz[NRC][NS];
 #pragma unroll
             for (int r = 0; r < NRC; ++r)
 #pragma unroll
                 for (int s = 0; s < NS; ++s)
                 {
-                    aG[r][s] = 0.0;
-                    aP1[r][s] = 0.0;
-                    aPx[r][s] = 0.0;
-                    aPy[r][s] = 0.0;
-                    aPz[r][s] = 0.0;
+                    aG[r][s] = R(0);
+                    aP1[r][s] = R(0);
+                    aPx[r][s] = R(0);
+                    aPy[r][s] = R(0);
+                    aPz[r][s] = R(0);
                 }
-            double eta2[NRC], etaN[NRC];
-            double const* Er[NRC];
+            R eta2[NRC], etaN[NRC];
+            R const* Er[NRC];
 #pragma unroll
             for (int r = 0; r < NRC; ++r)
             {
                 int const rr = min(rb + r, max(nr - 1, 0));
                 DevMember const& mm = M[g.mbeg + rr * NS];
-                eta2[r] = 2.0 * mm.eta;
-                etaN[r] = -mm.eta;
+                eta2[r] = R(2) * R(mm.eta);
+                etaN[r] = -R(mm.eta);
                 Er[r] = W.E + (long)mm.expIdx * capE;
             }
             if (valid && rb < nr)
             {
-                double const cr0 = invij * invij;  // 1 / r_ij^2
+                R const cr0 = invij * invij;  // 1 / r_ij^2
                 int const wb = it.pb >> 5;
                 int const we = (it.pe + 31) >> 5;
                 for (int w = wb; w < we; ++w)
@@ -683,22 +717,22 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                         {
                             if (k == t || !(W.d[k] < rc)) continue;
                         }
-                        double const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
-                        double const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1],
-                                               dr2[2] - dr1[2]};
-                        double const invik = W.inv[k];
-                        double const pfcik = W.fc[k];
-                        double const rinvijik = invij * invik;
-                        double const costijk = (dr1[0] * dr2[0] + dr1[1] * dr2[1]
-                                                + dr1[2] * dr2[2]) * rinvijik;
-                        double r2 = 0.0, pfc, pr1, pr3 = 0.0;
+                        R const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
+                        R const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1],
+                                          dr2[2] - dr1[2]};
+                        R const invik = W.inv[k];
+                        R const pfcik = W.fc[k];
+                        R const rinvijik = invij * invik;
+                        R const costijk = (dr1[0] * dr2[0] + dr1[1] * dr2[1]
+                                           + dr1[2] * dr2[2]) * rinvijik;
+                        R r2 = R(0), pfc, pr1, pr3 = R(0);
                         if (NARROW)
                         {
                             r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1]
                                + dr3[2] * dr3[2];
-                            double const invjk = rsqrt(r2);
-                            double pfcjk, pdfcjk;
-                            cutoffFdf<CT>(P, g, r2 * invjk, pfcjk, pdfcjk);
+                            R const invjk = mrsqrt(r2);
+                            R pfcjk, pdfcjk;
+                            cutoffFdf<R, CT>(P, g, r2 * invjk, pfcjk, pdfcjk);
                             pfc = pfcij * pfcik * pfcjk;
                             pr1 = pfcik * pfcjk * pdfcrij;
                             pr3 = pfcij * pfcik * pdfcjk * invjk;
@@ -708,14 +742,15 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                             pfc = pfcij * pfcik;
                             pr1 = pfcik * pdfcrij;
                         }
-                        double const X1 = pfc * (rinvijik - costijk * cr0);
-                        double const X3 = pfc * rinvijik;
-                        double A[NS], B[NS], Z1[NS], Z3[NS], pl[NS];
+                        R const X1 = pfc * (rinvijik - costijk * cr0);
+                        R const X3 = pfc * rinvijik;
+                        R A[NS], B[NS], Z1[NS], Z3[NS], pl[NS];
 #pragma unroll
                         for (int s = 0; s < NS; ++s)
                         {
-                            pl[s] = 1.0 + lam[s] * costijk;
-                            A[s] = (pl[s] <= 0.0) ? 0.0 : powInt(pl[s], zi[s] - 1);
+                            pl[s] = R(1) + lam[s] * costijk;
+                            A[s] = (pl[s] <= R(0)) ? R(0)
+                                                   : powInt(pl[s], zi[s] - 1);
                             B[s] = A[s] * pl[s] * pfc;
                             Z1[s] = zl[s] * X1;
                             Z3[s] = zl[s] * X3;
@@ -723,18 +758,18 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
 #pragma unroll
                         for (int r = 0; r < NRC; ++r)
                         {
-                            double vexp = Er[r][t] * Er[r][k];
-                            if (NARROW) vexp *= exp(etaN[r] * r2);
-                            double const e2p = eta2[r] * pfc;
-                            double const Y1 = pr1 - e2p;
-                            double const Y3 = NARROW ? e2p - pr3 : 0.0;
+                            R vexp = Er[r][t] * Er[r][k];
+                            if (NARROW) vexp *= mexp(etaN[r] * r2);
+                            R const e2p = eta2[r] * pfc;
+                            R const Y1 = pr1 - e2p;
+                            R const Y3 = NARROW ? e2p - pr3 : R(0);
 #pragma unroll
                             for (int s = 0; s < NS; ++s)
                             {
-                                double const wgt = vexp * A[s];
+                                R const wgt = vexp * A[s];
                                 aG[r][s] += vexp * B[s];
                                 aP1[r][s] += wgt * (Z1[s] + pl[s] * Y1);
-                                double const p3 = wgt * (Z3[s] + pl[s] * Y3);
+                                R const p3 = wgt * (Z3[s] + pl[s] * Y3);
                                 aPx[r][s] += p3 * dr3[0];
                                 aPy[r][s] += p3 * dr3[1];
                                 aPz[r][s] += p3 * dr3[2];
@@ -751,11 +786,11 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                     bool const has = active && (rb + r < nr);
                     DevMember const& mm =
                         M[g.mbeg + (has ? (rb + r) * NS + s : 0)];
-                    double const fn = mm.factorNorm;
-                    double const P1 = fn * aP1[r][s];
-                    double const sx = P1 * dr1[0];
-                    double const sy = P1 * dr1[1];
-                    double const sz = P1 * dr1[2];
+                    R const fn = R(mm.factorNorm);
+                    R const P1 = fn * aP1[r][s];
+                    R const sx = P1 * dr1[0];
+                    R const sy = P1 * dr1[1];
+                    R const sz = P1 * dr1[2];
                     if (derivatives && has)
                     {
                         long const sl = mm.slot[it.et];
@@ -763,17 +798,16 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                         out[(sl * 3 + 1) * cnt + t] = -(sy + fn * aPy[r][s]);
                         out[(sl * 3 + 2) * cnt + t] = -(sz + fn * aPz[r][s]);
                     }
-                    flushBySF(W, it.key, has ? (int)mm.sf : -1, 0.5 * aG[r][s],
-                              sx, sy,
-                              sz);
+                    flushBySF(W, it.key, has ? (int)mm.sf : -1,
+                              R(0.5) * aG[r][s], sx, sy, sz);
                 }
         }
     }
 }
 
-template <int CT, int NS, int NRC>
+template <typename R, int CT, int NS, int NRC>
 __global__ void __launch_bounds__(kThreads)
-sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
+sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 {
     extern __shared__ double smem0[];
     // Block-shared copy of the group and member tables (dynamically indexed
@@ -794,8 +828,7 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
         for (int k = threadIdx.x; k < wm; k += kThreads) dst[k] = src[k];
     }
     __syncthreads();
-    double* smem = reinterpret_cast<double*>(
-        reinterpret_cast<char*>(smem0) + tableBytes(ng, nm));
+    char* smem = reinterpret_cast<char*>(smem0) + tableBytes(ng, nm);
     DevGroup const* sG = tg;
     DevMember const* sM = tm;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
@@ -805,8 +838,8 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
     int const cap = L.cap;
     int const words = (cap + 31) >> 5;
     int const maxSF = P.maxSF;
-    double* wbase = smem + (long)warp * L.warpDoubles;
-    WarpMem W;
+    R* wbase = reinterpret_cast<R*>(smem + (long)warp * L.warpBytes);
+    WarpMem<R> W;
     W.dx = wbase;
     W.dy = W.dx + cap;
     W.dz = W.dy + cap;
@@ -817,9 +850,19 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
     W.E = W.dfcr + cap;
     W.wpG = W.E + (long)P.maxExp * cap;
     W.wpS = W.wpG + maxSF;
-    W.bits = reinterpret_cast<unsigned*>(W.wpS + 3 * maxSF);
-    W.cats = reinterpret_cast<Cat*>(W.bits + cap * words);
+    {
+        char* after = reinterpret_cast<char*>(W.wpS + 3 * maxSF);
+        long const off = (after - reinterpret_cast<char*>(wbase) + 15) / 16
+                       * 16;
+        W.bits = reinterpret_cast<unsigned*>(
+            reinterpret_cast<char*>(wbase) + off);
+        long const off2 = (off + 4L * cap * words + 15) / 16 * 16;
+        W.cats = reinterpret_cast<Cat*>(reinterpret_cast<char*>(wbase) + off2);
+    }
     W.sortCats = L.sortCats;
+    R* const outG = static_cast<R*>(L.G);
+    R* const outSelf = static_cast<R*>(L.dGdrSelf);
+    R* const outNbr = static_cast<R*>(L.dGdr);
 
     int const numElements = P.numElements;
     int const gw = blockIdx.x * kWarps + warp;
@@ -846,15 +889,15 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
         for (int t = lane; t < cnt; t += 32)
         {
             double const dd = L.dd[beg + t];
-            W.dx[t] = L.dx[beg + t];
-            W.dy[t] = L.dy[beg + t];
-            W.dz[t] = L.dz[beg + t];
-            W.d[t] = dd;
-            W.inv[t] = 1.0 / dd;
+            W.dx[t] = R(L.dx[beg + t]);
+            W.dy[t] = R(L.dy[beg + t]);
+            W.dz[t] = R(L.dz[beg + t]);
+            W.d[t] = R(dd);
+            W.inv[t] = R(1.0 / dd);
         }
-        for (int k = lane; k < 4 * maxSF; k += 32) W.wpG[k] = 0.0;
+        for (int k = lane; k < 4 * maxSF; k += 32) W.wpG[k] = R(0);
         __syncwarp();
-        double* out = L.dGdr + beg * (long)P.maxSlots * 3;
+        R* out = outNbr + beg * (long)P.maxSlots * 3;
         double fcRc = -1.0;
         double bitsRc = -1.0;
         int const gb = P.groupBeg[ec], ge = P.groupBeg[ec + 1];
@@ -874,8 +917,8 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
             {
                 for (int t = lane; t < cnt; t += 32)
                 {
-                    double fc, dfc;
-                    cutoffFdf<CT>(P, h, W.d[t], fc, dfc);
+                    R fc, dfc;
+                    cutoffFdf<R, CT>(P, h, W.d[t], fc, dfc);
                     W.fc[t] = fc;
                     W.dfcr[t] = dfc * W.inv[t];
                 }
@@ -884,10 +927,10 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
             if (h.type == 3 && h.rc != bitsRc)
             {
                 // Narrow-angular validity: k != t, r_ik < rc, r_jk^2 < rc^2.
-                double const rc = h.rc, rc2 = h.rc2;
+                R const rc = R(h.rc), rc2 = R(h.rc2);
                 for (int t = lane; t < cnt; t += 32)
                 {
-                    double const x = W.dx[t], y = W.dy[t], z = W.dz[t];
+                    R const x = W.dx[t], y = W.dy[t], z = W.dz[t];
                     for (int w = 0; w < words; ++w)
                     {
                         unsigned m = 0u;
@@ -895,9 +938,9 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
                         int const ke = min(cnt, kb + 32);
                         for (int k = kb; k < ke; ++k)
                         {
-                            double const a = W.dx[k] - x;
-                            double const b = W.dy[k] - y;
-                            double const c = W.dz[k] - z;
+                            R const a = W.dx[k] - x;
+                            R const b = W.dy[k] - y;
+                            R const c = W.dz[k] - z;
                             bool const ok = (k != t) && (W.d[k] < rc)
                                           && (a * a + b * b + c * c < rc2);
                             m |= (ok ? 1u : 0u) << (k - kb);
@@ -918,33 +961,34 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
                     {
                         DevMember const& mm = sM[g.mbeg + l];
                         if (!mm.calcExp) continue;
-                        double* E = W.E + (long)mm.expIdx * cap;
+                        R* E = W.E + (long)mm.expIdx * cap;
+                        R const eta = R(mm.eta), rs = R(mm.rs);
                         for (int t = lane; t < cnt; t += 32)
                         {
-                            double const rr = W.d[t] - mm.rs;
-                            E[t] = exp(-mm.eta * rr * rr);
+                            R const rr = W.d[t] - rs;
+                            E[t] = mexp(-eta * rr * rr);
                         }
                     }
                 }
             }
             __syncwarp();
             if (h.type == 2)
-                radialSegment<kGenericChunk>(sG, sM, g0, g1, eb, cnt, W, out,
-                                             L.derivatives);
+                radialSegment<R, kGenericChunk>(sG, sM, g0, g1, eb, cnt, W,
+                                                out, L.derivatives);
             else if (fast && h.type == 3)
-                angularFast<CT, NS, NRC, true>(P, sG, sM, g0, g1, eb, cnt,
-                                               words, cap, W, out,
-                                               L.derivatives);
+                angularFast<R, CT, NS, NRC, true>(P, sG, sM, g0, g1, eb, cnt,
+                                                  words, cap, W, out,
+                                                  L.derivatives);
             else if (fast)
-                angularFast<CT, NS, NRC, false>(P, sG, sM, g0, g1, eb, cnt,
-                                                words, cap, W, out,
-                                                L.derivatives);
+                angularFast<R, CT, NS, NRC, false>(P, sG, sM, g0, g1, eb, cnt,
+                                                   words, cap, W, out,
+                                                   L.derivatives);
             else if (h.type == 3)
-                angularGeneric<CT, kGenericChunk, true>(
+                angularGeneric<R, CT, kGenericChunk, true>(
                     P, sG, sM, g0, g1, eb, cnt, words, cap, W, out,
                     L.derivatives);
             else
-                angularGeneric<CT, kGenericChunk, false>(
+                angularGeneric<R, CT, kGenericChunk, false>(
                     P, sG, sM, g0, g1, eb, cnt, words, cap, W, out,
                     L.derivatives);
             __syncwarp();
@@ -956,10 +1000,11 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
         for (int s = lane; s < nsf; s += 32)
         {
             SFScale const q = sc[s];
-            L.G[(long)i * maxSF + s] = q.smin + q.b * (q.q * W.wpG[s] - q.shift);
+            outG[(long)i * maxSF + s] =
+                R(q.smin + q.b * (q.q * (double)W.wpG[s] - q.shift));
             if (L.derivatives)
             {
-                double* o = L.dGdrSelf + ((long)i * maxSF + s) * 3;
+                R* o = outSelf + ((long)i * maxSF + s) * 3;
                 o[0] = W.wpS[3 * s + 0];
                 o[1] = W.wpS[3 * s + 1];
                 o[2] = W.wpS[3 * s + 2];
@@ -970,51 +1015,51 @@ sfFp64Kernel(__grid_constant__ SFParams const P, SFLaunch const L)
 }
 
 // Launch and occupancy helpers for one cutoff type; variant = (NS, NRC).
-template <int CT, int NS, int NRC>
+template <typename R, int CT, int NS, int NRC>
 void launchVariant(SFParams const& P, SFLaunch const& L, std::size_t shm,
                    cudaStream_t s)
 {
-    cudaFuncSetAttribute(sfFp64Kernel<CT, NS, NRC>,
+    cudaFuncSetAttribute(sfKernel<R, CT, NS, NRC>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    sfFp64Kernel<CT, NS, NRC><<<L.grid, kThreads, shm, s>>>(P, L);
+    sfKernel<R, CT, NS, NRC><<<L.grid, kThreads, shm, s>>>(P, L);
 }
 
-template <int CT, int NS, int NRC>
+template <typename R, int CT, int NS, int NRC>
 int blocksVariant(std::size_t shm)
 {
-    cudaFuncSetAttribute(sfFp64Kernel<CT, NS, NRC>,
+    cudaFuncSetAttribute(sfKernel<R, CT, NS, NRC>,
                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
     int blocks = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &blocks, sfFp64Kernel<CT, NS, NRC>, kThreads, shm) != cudaSuccess
+            &blocks, sfKernel<R, CT, NS, NRC>, kThreads, shm) != cudaSuccess
         || blocks < 1)
         blocks = 1;
     return blocks;
 }
 
 // Variants: 0 = (NS 4, NRC 3), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
-template <int CT>
+template <typename R, int CT>
 void launchForCT(SFParams const& P, SFLaunch const& L, std::size_t shm,
                  cudaStream_t s, int variant)
 {
     switch (variant)
     {
-    case 1: launchVariant<CT, 4, 1>(P, L, shm, s); break;
-    case 2: launchVariant<CT, 8, 1>(P, L, shm, s); break;
-    case 3: launchVariant<CT, 8, 2>(P, L, shm, s); break;
-    default: launchVariant<CT, 4, 3>(P, L, shm, s); break;
+    case 1: launchVariant<R, CT, 4, 1>(P, L, shm, s); break;
+    case 2: launchVariant<R, CT, 8, 1>(P, L, shm, s); break;
+    case 3: launchVariant<R, CT, 8, 2>(P, L, shm, s); break;
+    default: launchVariant<R, CT, 4, 3>(P, L, shm, s); break;
     }
 }
 
-template <int CT>
+template <typename R, int CT>
 int blocksForCT(std::size_t shm, int variant)
 {
     switch (variant)
     {
-    case 1: return blocksVariant<CT, 4, 1>(shm);
-    case 2: return blocksVariant<CT, 8, 1>(shm);
-    case 3: return blocksVariant<CT, 8, 2>(shm);
-    default: return blocksVariant<CT, 4, 3>(shm);
+    case 1: return blocksVariant<R, CT, 4, 1>(shm);
+    case 2: return blocksVariant<R, CT, 8, 1>(shm);
+    case 3: return blocksVariant<R, CT, 8, 2>(shm);
+    default: return blocksVariant<R, CT, 4, 3>(shm);
     }
 }
 

@@ -218,6 +218,26 @@ class Mode:
         self._check(self._L.n2p2b_set_stream(
             self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
+    _PRECISIONS = {"fp64": _capi.PRECISION_FP64,
+                   "mixed": _capi.PRECISION_MIXED,
+                   "bf16": _capi.PRECISION_BF16}
+
+    def set_precision(self, mode: str):
+        """"fp64" (plain form, default), "mixed" (FP32 symmetry functions;
+        tensor-core NNs on BF16 high/low operand pairs with FP32
+        accumulation) or "bf16" (the same with single BF16 operands).  The
+        mixed forms keep FP64 displacements, energy sum and force
+        accumulation."""
+        if mode not in self._PRECISIONS:
+            raise ValueError(f"unknown precision {mode!r}")
+        self._check(self._L.n2p2b_set_precision(self._h,
+                                                self._PRECISIONS[mode]))
+
+    @property
+    def precision(self) -> str:
+        m = self._L.n2p2b_get_precision(self._h)
+        return {v: k for k, v in self._PRECISIONS.items()}[m]
+
     # ---- results -----------------------------------------------------------
     @property
     def energy(self) -> float:
