@@ -11,7 +11,11 @@ functions per element (radial + narrow angular, cos cutoff 12 bohr), NN
 h2o_52).  One step = one frame through neighbor list, symmetry functions +
 dG/dr, atomic NNs + dE/dG, energy and forces, all in FP64.
 
-Metric: E+F atoms/s (higher is better).
+Metric: E+F atoms/s (higher is better).  `value` and `e2e` are the plain
+FP64 form; `forms` adds, on the same frames, the mixed-precision forms (FP32
+symmetry functions, tensor-core BF16 networks) for this potential and for
+the wider 92-SF / 64-64-64 potential, each with its speed-up over FP64 and
+its energy-per-atom and force RMSE against the FP64 form.
   value : device-resident frames (HBM), K steps between CUDA events on the
           library's stream, max over ranks; frames cycle through 100
           distinct coordinate sets and the per-frame working set (dG/dr,
@@ -45,12 +49,20 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-POT = os.path.join(ROOT, "tests", "golden", "potentials", "h2o_52")
+POT_DIR = os.path.join(ROOT, "tests", "golden", "potentials")
+POT = os.path.join(POT_DIR, "h2o_52")
+STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
+          "forces")
+# DRAM bytes (read + write) of one symmetry-function launch on this
+# workload, from the ncu capture summarized under profiles/ (None until a
+# capture of the current kernel exists).
+SF_TRAFFIC_BYTES = None
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
 SIGMA = 0.1
-METRIC = "E+F atoms/s (plain FP64, 24,576-atom water box)"
+METRIC = ("E+F atoms/s on 1 B200: plain FP64 vs BF16 / gated student at "
+          "stated force RMSE")
 
 
 def args():
@@ -61,6 +73,8 @@ def args():
     a.add_argument("--impl", choices=["ours", "reference"], default="ours")
     a.add_argument("--frames", type=int, default=N_FRAMES)
     a.add_argument("--no-cpu-baseline", action="store_true")
+    a.add_argument("--no-forms", action="store_true",
+                   help="skip the mixed-precision comparison")
     return a.parse_args()
 
 
@@ -235,6 +249,7 @@ def cpu_baseline(frames, box, elem, reps=1):
     oref.REF_LIB = lib
     threads = os.cpu_count() or 1
     m = oref.RefModel(POT)
+    m.setup_statistics()
     m.set_structure(frames[0], elem, box)
     t = m.time_stages(threads=threads, reps=reps)
     total = float(t.sum())
@@ -263,6 +278,7 @@ def run_reference(a):
     box, frames, elem = workload(0, min(a.frames, max(a.steps, 1) + 1))
     threads = os.cpu_count() or 1
     m = oref.RefModel(POT)
+    m.setup_statistics()   # no extrapolation-warning output, as our arm
     # one warm-up frame (a CPU path has no device warm-up to amortize)
     m.set_structure(frames[0], elem, box)
     t0 = time.perf_counter()
@@ -299,6 +315,96 @@ def run_reference(a):
 # ---------------------------------------------------------------------------
 # our arm
 # ---------------------------------------------------------------------------
+def _time_steps(p, frames_dev, steps, stream, lib):
+    """Device time of `steps` evaluations on device-resident frames (CUDA
+    events on the library's stream) and the number of launches."""
+    import torch
+    F = len(frames_dev)
+    l0 = lib.n2p2b_kernel_launch_count()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for s in range(steps):
+        p.set_positions(frames_dev[s % F])
+        p.evaluate_async(True)
+    ev1.record(stream)
+    p.finish()
+    return ev0.elapsed_time(ev1) / 1e3, int(lib.n2p2b_kernel_launch_count()
+                                            - l0)
+
+
+def _stage_ms(p, frames_dev, steps):
+    F = len(frames_dev)
+    p.set_profiling(True)
+    p.stage_times(reset=True)
+    for s in range(steps):
+        p.set_positions(frames_dev[s % F])
+        p.evaluate_async(True)
+    p.finish()
+    ms, runs = p.stage_times(reset=True)
+    p.set_profiling(False)
+    return [x / max(runs, 1) for x in ms]
+
+
+def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
+    """Plain FP64 vs the mixed forms on the same 24,576-atom frames, for the
+    52-SF potential and the wider 92-SF / 64-64-64 softplus potential.
+    Accuracy is measured against the FP64 form on three frames (the FP64
+    form equals the reference to 1e-10, tests/test_gpu_parity.py)."""
+    from n2p2_b200.mode import Prediction
+    n = len(elem)
+    out = {}
+    for pot in ("h2o_52", "h2o_92"):
+        p = Prediction(os.path.join(POT_DIR, pot), device=local)
+        p.setup()
+        p.setup_symmetry_function_statistics(False, False, False, False)
+        p.set_stream(stream.cuda_stream)
+        p.set_structure(frames[0], elem, box)
+        ref = None
+        for prec in ("fp64", "mixed", "bf16"):
+            p.set_precision(prec)
+            p.set_positions(frames[0])
+            p.evaluate_nnp(True)
+            for s in range(3):
+                p.set_positions(dev_frames[s])
+                p.evaluate_async(True)
+            p.finish()
+            t, launches = _time_steps(p, dev_frames, steps, stream, lib)
+            stage = _stage_ms(p, dev_frames, min(steps, 10))
+            acc = []
+            for s in range(3):
+                p.set_positions(frames[s])
+                p.evaluate_nnp(True)
+                acc.append((p.energy, p.forces().copy()))
+            entry = {"value": n * steps / t, "unit": "atoms/s",
+                     "ms_per_step": 1e3 * t / steps, "steps": steps,
+                     "stage_ms_per_step": dict(zip(STAGES, stage))}
+            if prec == "fp64":
+                ref = acc
+            else:
+                de = [(e - e0) / n for (e, _), (e0, _) in zip(acc, ref)]
+                df = np.concatenate([(f - f0).ravel()
+                                     for (_, f), (_, f0) in zip(acc, ref)])
+                entry["energy_per_atom_rmse_vs_fp64"] = float(
+                    np.sqrt(np.mean(np.square(de))))
+                entry["force_rmse_vs_fp64"] = float(
+                    np.sqrt(np.mean(np.square(df))))
+                entry["speedup_vs_fp64"] = (
+                    entry["value"] / out[pot]["fp64"]["value"])
+            out.setdefault(pot, {})[prec] = entry
+        out[pot]["force_rms"] = float(np.sqrt(np.mean(np.square(ref[0][1]))))
+        p.close()
+    out["targets"] = {"energy_per_atom_rmse": 1e-4, "force_rmse": 5e-3,
+                      "units": "potential energy units; energy / bohr"}
+    out["forms"] = {
+        "fp64": "plain form, everything FP64",
+        "mixed": "FP32 symmetry functions + dG/dr; NN on tcgen05 with BF16 "
+                 "hi/lo operand pairs (3 MMAs per step), FP32 accumulation; "
+                 "FP64 displacements, energy sum, force accumulation",
+        "bf16": "as mixed with single BF16 operands (1 MMA per step)"}
+    return out
+
+
 def run_ours(a):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -325,6 +431,9 @@ def run_ours(a):
 
     p = Prediction(POT, device=local)
     p.setup()
+    # Hot path only: no extrapolation-warning output (the reference arm runs
+    # with the same setting).
+    p.setup_symmetry_function_statistics(False, False, False, False)
     p.set_stream(stream.cuda_stream)
     p.set_structure(host_frames[0].numpy(), elem, box)
     p.evaluate_nnp(True)          # sizes all buffers (capacity known)
@@ -351,18 +460,9 @@ def run_ours(a):
     with ClockSampler(local) as clocks:
         # ---- value: device-resident frames -------------------------------
         barrier()
-        l0 = lib.n2p2b_kernel_launch_count()
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record(stream)
-        for s in range(a.steps):
-            p.set_positions(dev_frames[s % F])
-            p.evaluate_async(True)
-        ev1.record(stream)
-        p.finish()
+        t_dev, launches = _time_steps(p, dev_frames, a.steps, stream, lib)
         barrier()
-        launches = int(lib.n2p2b_kernel_launch_count() - l0)
-        t_dev = max_over_ranks(ev0.elapsed_time(ev1) / 1e3)
+        t_dev = max_over_ranks(t_dev)
 
         # ---- e2e: host buffers through the C-ABI -------------------------
         barrier()
@@ -378,14 +478,13 @@ def run_ours(a):
         t_e2e = max_over_ranks(time.perf_counter() - t0)
 
         # ---- profiled pass: per-stage device time -------------------------
-        p.set_profiling(True)
-        p.stage_times(reset=True)
-        for s in range(a.steps):
-            p.set_positions(dev_frames[s % F])
-            p.evaluate_async(True)
-        p.finish()
-        stage_ms, runs = p.stage_times(reset=True)
-        p.set_profiling(False)
+        per = _stage_ms(p, dev_frames, a.steps)
+
+        # ---- the other forms (one GPU only) -------------------------------
+        forms = None
+        if world == 1 and not a.no_forms:
+            forms = measure_forms(box, frames, elem, dev_frames, stream, lib,
+                                  min(a.steps, 50), local)
 
     if dist is not None:
         dist.barrier()
@@ -403,7 +502,6 @@ def run_ours(a):
     p.evaluate_nnp(True)
     cnt, index, dr, d = p.neighbor_list()
     wm = work_model(cnt, index, dr, d, elem)
-    per = [x / max(runs, 1) for x in stage_ms]
     sf_s = per[1] / 1e3
     hbm_peak, peak_kind = measured_peaks()
     gbs = wm["bytes_sf"] / sf_s / 1e9
@@ -423,17 +521,15 @@ def run_ours(a):
                 "path": "n2p2b_set_positions(host) + n2p2b_evaluate + "
                         "n2p2b_get_forces(host) + n2p2b_get_energy"},
         "gpu_launches": launches,
-        "stage_ms_per_step": {"neighbor_list": per[0],
-                              "symmetry_functions": per[1],
-                              "neural_networks": per[2], "energy": per[3],
-                              "forces": per[4]},
-        "roofline": {"kernel": "sfFp64Kernel (symmetry functions + dG/dr)",
+        "stage_ms_per_step": dict(zip(STAGES, per)),
+        "roofline": {"kernel": "sfKernel<double> (symmetry functions + "
+                               "dG/dr)",
                      "bound": "hbm", "achieved": gbs, "peak": hbm_peak,
                      "unit": "GB/s", "frac": gbs / hbm_peak,
                      "peak_source": peak_kind,
-                     "traffic": None,
+                     "traffic": SF_TRAFFIC_BYTES,
                      "algorithmic_bytes_per_launch": wm["bytes_sf"]},
-        "roofline_fp64": {"kernel": "sfFp64Kernel", "achieved": sf_tflops,
+        "roofline_fp64": {"kernel": "sfKernel<double>", "achieved": sf_tflops,
                           "peak": fp64_peak, "unit": "TFLOP/s",
                           "frac": sf_tflops / fp64_peak,
                           "peak_source": "cuBLAS DGEMM 8192^3 measured here",
@@ -442,6 +538,8 @@ def run_ours(a):
         "energy_last_frame": energy,
         "clocks": clocks.summary(),
     }
+    if forms is not None:
+        line["forms"] = forms
     if not a.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(frames, box, elem)
     print(json.dumps(line))

@@ -39,6 +39,10 @@ typedef struct n2p2b_context n2p2b_context;
 #define N2P2B_ERR_CAPACITY      -4  /* capacity exceeded and not recoverable */
 #define N2P2B_ERR_STATE         -5  /* call out of order (no setup/structure)*/
 #define N2P2B_ERR_INTERNAL      -6  /* broken invariant (reported, not hit)  */
+#define N2P2B_ERR_EXTRAPOLATION -7  /* extrapolation warning with "stop on
+                                       warning" set (the reference's
+                                       std::out_of_range); results are
+                                       computed all the same               */
 
 /* Where an array argument lives. */
 #define N2P2B_HOST               0
@@ -164,6 +168,27 @@ int n2p2b_evaluate(n2p2b_context* ctx, int use_forces);
 int n2p2b_evaluate_async(n2p2b_context* ctx, int use_forces);
 /* Waits for the context's stream and reports capacity / invariant flags. */
 int n2p2b_finish(n2p2b_context* ctx);
+
+/* ---- extrapolation warnings (Element::updateSymmetryFunctionStatistics) */
+
+/* Mode::setupSymmetryFunctionStatistics (libnnp/Mode.cpp:1103-1137): after
+ * every symmetry-function calculation, count the symmetry functions whose
+ * unscaled value lies outside scaling.data's [Gmin, Gmax] by more than
+ * 1000 DBL_EPSILON (libnnp/Element.cpp:462-541).  write_ew prints the
+ * reference's "### NNP EXTRAPOLATION WARNING ###" lines to stderr;
+ * stop_on_ew makes the evaluation return N2P2B_ERR_EXTRAPOLATION.
+ * collect_statistics (the SF statistics of the training tools) is not
+ * supported and must be 0. */
+int n2p2b_setup_symmetry_function_statistics(n2p2b_context* ctx,
+                                             int collect_statistics,
+                                             int collect_ew, int write_ew,
+                                             int stop_on_ew);
+/* Mode::getNumExtrapolationWarnings / resetExtrapolationWarnings
+ * (libnnp/Mode.h:478-486): warnings counted since the last reset. */
+int64_t n2p2b_get_num_extrapolation_warnings(const n2p2b_context* ctx);
+int     n2p2b_reset_extrapolation_warnings(n2p2b_context* ctx);
+/* Warnings per atom of the last evaluation (num_atoms ints). */
+int     n2p2b_get_extrapolation_counts(n2p2b_context* ctx, int32_t* counts);
 
 /* ---- results ---------------------------------------------------------- */
 

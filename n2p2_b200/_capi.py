@@ -19,6 +19,7 @@ ERR_CUDA = -3
 ERR_CAPACITY = -4
 ERR_STATE = -5
 ERR_INTERNAL = -6
+ERR_EXTRAPOLATION = -7
 HOST = 0
 DEVICE = 1
 REMAP = 1
@@ -39,6 +40,11 @@ SIGNATURES = {
     "n2p2b_set_stream": (C.c_int, [_vp, _vp]),
     "n2p2b_set_precision": (C.c_int, [_vp, C.c_int]),
     "n2p2b_get_precision": (C.c_int, [_vp]),
+    "n2p2b_setup_symmetry_function_statistics": (
+        C.c_int, [_vp, C.c_int, C.c_int, C.c_int, C.c_int]),
+    "n2p2b_get_num_extrapolation_warnings": (C.c_int64, [_vp]),
+    "n2p2b_reset_extrapolation_warnings": (C.c_int, [_vp]),
+    "n2p2b_get_extrapolation_counts": (C.c_int, [_vp, _i32p]),
     "n2p2b_load_settings_file": (C.c_int, [_vp, C.c_char_p]),
     "n2p2b_setup_generic": (C.c_int, [_vp]),
     "n2p2b_setup_symmetry_function_scaling": (C.c_int, [_vp, C.c_char_p]),

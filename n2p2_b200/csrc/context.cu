@@ -10,6 +10,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cfloat>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -35,6 +36,11 @@ struct CapacityError : std::runtime_error
 };
 
 struct StateError : std::runtime_error
+{
+    using std::runtime_error::runtime_error;
+};
+
+struct ExtrapolationError : std::runtime_error
 {
     using std::runtime_error::runtime_error;
 };
@@ -196,6 +202,13 @@ struct n2p2b_context
     DevBuf       tcW[2], tcF[2];
     int          tileBeg[kMaxElem + 1] = {};
     int          tcGrid[2] = {0, 0};
+    // Extrapolation warnings (Mode::setupSymmetryFunctionStatistics).
+    bool         ewCheck = false, ewWrite = false, ewStop = false;
+    long         ewTotal = 0;
+    bool         haveEW = false;
+    std::vector<Range> ewRangeHost;
+    std::vector<SFScale> sfScaleHost;
+    DevBuf       ewRange, ewPerAtom;
 
     // Structure.
     long         n = 0;
@@ -295,7 +308,7 @@ struct n2p2b_context
         for (auto& se : freeEvents)
             for (auto& e : se.ev) cudaEventDestroy(e);
         for (DevBuf* b : {&sfScale, &nnW, &slotSF, &tcW[0], &tcF[0], &tcW[1],
-                          &tcF[1], &posIn, &pos, &elem,
+                          &tcF[1], &ewRange, &ewPerAtom, &posIn, &pos, &elem,
                           &atomsByElem, &cellOf, &cellCount, &cellFill,
                           &cellStart, &cellAtoms, &cellStatus, &nbrCount,
                           &nbrCountElem, &nbrOff, &keyTmp, &key, &nbrIdx,
@@ -372,6 +385,7 @@ struct n2p2b_context
         sfp.E = std::exp(1.0);
         sfp.TANH_PRE = std::pow((sfp.E + 1 / sfp.E) / (sfp.E - 1 / sfp.E), 3);
         std::vector<SFScale> scale((std::size_t)ne * maxSF, SFScale{0, 1, 0, 1});
+        ewRangeHost.assign((std::size_t)ne * maxSF, Range{0.0, 0.0});
         std::vector<int16_t> slotTab((std::size_t)kMaxElem * kMaxElem
                                      * std::max(maxSlots, 1), (int16_t)-1);
         int gi = 0, mi = 0;
@@ -427,6 +441,8 @@ struct n2p2b_context
                         m.slot[f] = (f < ne) ? (int16_t)s.indexPerElement[f]
                                              : (int16_t)-1;
                     SFScale& q = scale[(std::size_t)e * maxSF + s.index];
+                    ewRangeHost[(std::size_t)e * maxSF + s.index] =
+                        Range{s.Gmin, s.Gmax};
                     if (g.type == 2)
                     {
                         m.factorNorm = s.scalingFactor;
@@ -515,6 +531,11 @@ struct n2p2b_context
         sfScale.ensure(sizeof(SFScale) * scale.size());
         ck(cudaMemcpy(sfScale.p, scale.data(), sizeof(SFScale) * scale.size(),
                       cudaMemcpyHostToDevice), "copy SF scaling");
+        sfScaleHost = scale;
+        ewRange.ensure(sizeof(Range) * ewRangeHost.size());
+        ck(cudaMemcpy(ewRange.p, ewRangeHost.data(),
+                      sizeof(Range) * ewRangeHost.size(),
+                      cudaMemcpyHostToDevice), "copy SF ranges");
         nnW.ensure(sizeof(double) * blob.size());
         ck(cudaMemcpy(nnW.p, blob.data(), sizeof(double) * blob.size(),
                       cudaMemcpyHostToDevice), "copy NN weights");
@@ -695,6 +716,7 @@ struct n2p2b_context
         dEdG.ensure(realBytes() * n * maxSF);
         dGdrSelf.ensure(realBytes() * n * maxSF * 3);
         Ei.ensure(sizeof(double) * n);
+        ewPerAtom.ensure(sizeof(int) * n);
         selfF.ensure(sizeof(double) * n * 3);
         F.ensure(sizeof(double) * n * 3);
         energyOut.ensure(sizeof(double) * 2);
@@ -871,6 +893,74 @@ struct n2p2b_context
         launchSymmetryFunctions(sfp, L, stream);
     }
 
+    // Element::updateSymmetryFunctionStatistics for every atom.
+    void enqueueEW()
+    {
+        EWLaunch L;
+        L.n = (int)n;
+        L.maxSF = maxSF;
+        L.precision = precision;
+        for (int e = 0; e < pot.numElements(); ++e) L.numSF[e] = sfp.numSF[e];
+        L.elem = elem.as<int>();
+        L.G = G.p;
+        L.scale = sfScale.as<SFScale>();
+        L.range = ewRange.as<Range>();
+        L.perAtom = ewPerAtom.as<int>();
+        L.status = status.as<int>();
+        launchExtrapolationCheck(L, stream);
+    }
+
+    // Accounts the warnings of a finished evaluation (status words read).
+    void accountEW()
+    {
+        int const cnt = statusHost[ST_EW_COUNT];
+        haveEW = true;
+        ewTotal += cnt;
+        if (cnt <= 0) return;
+        std::string first;
+        if (ewWrite || ewStop) first = ewLines(ewWrite);
+        if (ewStop)
+            throw ExtrapolationError(first + "ERROR: Symmetry function value "
+                                     "out of range.\n");
+    }
+
+    // The reference's warning lines (Element.cpp:505-518) for the last
+    // evaluation; prints all of them when `print`, returns the first.
+    std::string ewLines(bool print)
+    {
+        std::vector<int> per(n);
+        ck(cudaMemcpy(per.data(), ewPerAtom.p, sizeof(int) * n,
+                      cudaMemcpyDeviceToHost), "read warnings");
+        std::vector<double> const g = readReal(G, (std::size_t)n * maxSF);
+        std::string first;
+        double const eps = 1000.0 * DBL_EPSILON;
+        for (long i = 0; i < n; ++i)
+        {
+            if (per[i] == 0) continue;
+            int const e = elemHost[i];
+            Element const& el = pot.elements[e];
+            for (std::size_t s = 0; s < el.sfs.size(); ++s)
+            {
+                SFScale const& q = sfScaleHost[(std::size_t)e * maxSF + s];
+                Range const& r = ewRangeHost[(std::size_t)e * maxSF + s];
+                double const v = (g[(std::size_t)i * maxSF + s] - q.smin) / q.b
+                               + q.shift;
+                if (!(v + eps < r.lo || v - eps > r.hi)) continue;
+                char buf[256];
+                std::snprintf(buf, sizeof(buf),
+                              "### NNP EXTRAPOLATION WARNING ### STRUCTURE: "
+                              "%6zu ATOM: %9ld ELEMENT: %2s SYMFUNC: %4zu "
+                              "TYPE: %2d VALUE: %10.3E MIN: %10.3E MAX: "
+                              "%10.3E\n", (std::size_t)0, i,
+                              el.symbol.c_str(), s + 1, el.sfs[s].type, v,
+                              r.lo, r.hi);
+                if (first.empty()) first = buf;
+                if (print) std::fputs(buf, stderr);
+            }
+        }
+        return first;
+    }
+
     void enqueueNN(bool deriv)
     {
         if (precision != PREC_FP64)
@@ -1012,7 +1102,12 @@ struct n2p2b_context
             if (sizing) st = 1;
             beginProfile();
             if (st & 1) { enqueueNL(); mark(1); }
-            if (st & 2) { enqueueSF(sfDeriv); mark(2); }
+            if (st & 2)
+            {
+                enqueueSF(sfDeriv);
+                if (ewCheck) enqueueEW();
+                mark(2);
+            }
             if (st & 4) { enqueueNN(nnDeriv); mark(3); }
             if (st & 8) { enqueueEnergy(); mark(4); }
             if (st & 16) { enqueueForces(); mark(5); }
@@ -1051,6 +1146,7 @@ struct n2p2b_context
             if (stages & 4) { haveNN = true; haveNNDeriv = nnDeriv; }
             if (stages & 8) haveE = true;
             if (stages & 16) haveF = true;
+            if ((stages & 2) && ewCheck) accountEW();
             return;
         }
         throw CapacityError("ERROR: Capacity retries exhausted.\n");
@@ -1069,6 +1165,7 @@ struct n2p2b_context
         enqueueNL();
         mark(1);
         enqueueSF(forces);
+        if (ewCheck) enqueueEW();
         mark(2);
         enqueueNN(forces);
         mark(3);
@@ -1097,6 +1194,7 @@ struct n2p2b_context
             throw CudaError("ERROR: A tensor-core wait of the NN kernel gave "
                             "up; results are invalid.\n");
         haveNL = haveSF = haveNN = haveE = true;
+        if (ewCheck) accountEW();
         return 0;
     }
 
@@ -1161,6 +1259,11 @@ int guarded(n2p2b_context* ctx, F&& f)
     {
         ctx->error = e.what();
         return N2P2B_ERR_STATE;
+    }
+    catch (ExtrapolationError const& e)
+    {
+        ctx->error = e.what();
+        return N2P2B_ERR_EXTRAPOLATION;
     }
     catch (std::invalid_argument const& e)
     {
@@ -1286,6 +1389,46 @@ int n2p2b_set_precision(n2p2b_context* ctx, int mode)
 int n2p2b_get_precision(n2p2b_context const* ctx)
 {
     return ctx ? ctx->precision : N2P2B_ERR_ARGUMENT;
+}
+
+int n2p2b_setup_symmetry_function_statistics(n2p2b_context* ctx,
+                                             int collect_statistics,
+                                             int collect_ew, int write_ew,
+                                             int stop_on_ew)
+{
+    return guarded(ctx, [&] {
+        if (collect_statistics)
+            throw std::invalid_argument("ERROR: Symmetry-function statistics "
+                                        "collection is not supported.\n");
+        ctx->ewCheck = collect_ew || write_ew || stop_on_ew;
+        ctx->ewWrite = write_ew != 0;
+        ctx->ewStop = stop_on_ew != 0;
+        ctx->invalidate();
+    });
+}
+
+int64_t n2p2b_get_num_extrapolation_warnings(n2p2b_context const* ctx)
+{
+    return ctx ? ctx->ewTotal : 0;
+}
+
+int n2p2b_reset_extrapolation_warnings(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] { ctx->ewTotal = 0; });
+}
+
+int n2p2b_get_extrapolation_counts(n2p2b_context* ctx, int32_t* counts)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveEW || !ctx->ewCheck)
+            throw StateError("ERROR: No extrapolation check ran (enable it "
+                             "with n2p2b_setup_symmetry_function_statistics)."
+                             "\n");
+        if (counts == nullptr) throw std::invalid_argument("ERROR: counts");
+        ctx->activate();
+        ck(cudaMemcpy(counts, ctx->ewPerAtom.p, sizeof(int32_t) * ctx->n,
+                      cudaMemcpyDeviceToHost), "read warnings");
+    });
 }
 
 int n2p2b_load_settings_file(n2p2b_context* ctx, char const* path)

@@ -203,6 +203,31 @@ bool tcBuild(NNParams const& nn, std::vector<double> const& blob, int split,
 // memory limits).
 int tcBlocksPerSM(TcNNParams const& P);
 
+// Extrapolation test / student gate (kernels_gate.cu).
+struct Range
+{
+    double lo, hi;    // allowed range of the unscaled symmetry function
+};
+
+struct EWLaunch
+{
+    int            n = 0;
+    int            maxSF = 0;
+    int            precision = PREC_FP64;   // type of G
+    int            numSF[kMaxElem] = {};
+    int const*     elem = nullptr;
+    void const*    G = nullptr;             // [n][maxSF] scaled values
+    SFScale const* scale = nullptr;         // [element][maxSF]
+    Range const*   range = nullptr;         // [element][maxSF]
+    int*           perAtom = nullptr;       // [n] warnings per atom, or null
+    int*           list = nullptr;          // atoms with warnings, per
+    int*           listCount = nullptr;     // element at listStart[e]
+    int            listStart[kMaxElem] = {};
+    int*           status = nullptr;        // ST_EW_COUNT accumulates
+};
+
+void launchExtrapolationCheck(EWLaunch const& L, cudaStream_t s);
+
 // Forces (chain rule) and energy.
 struct ForceLaunch
 {

@@ -35,6 +35,11 @@ class StateError(N2P2Error):
     pass
 
 
+class ExtrapolationError(N2P2Error, IndexError):
+    """An extrapolation warning with stop-on-warning set (the reference
+    throws std::out_of_range); the evaluation's results are complete."""
+
+
 def _is_device_tensor(a) -> bool:
     return hasattr(a, "is_cuda") and bool(a.is_cuda)
 
@@ -83,6 +88,8 @@ class Mode:
             raise CapacityError(rc, msg)
         if rc == _capi.ERR_STATE:
             raise StateError(rc, msg)
+        if rc == _capi.ERR_EXTRAPOLATION:
+            raise ExtrapolationError(rc, msg)
         if rc == _capi.ERR_ARGUMENT:
             raise ValueError(msg)
         raise N2P2Error(rc, msg)
@@ -218,6 +225,30 @@ class Mode:
         self._check(self._L.n2p2b_set_stream(
             self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
 
+    # ---- extrapolation warnings (Mode.h:209-224, 478-486) ----------------
+    def setup_symmetry_function_statistics(self, collect_statistics=False,
+                                           collect_extrapolation_warnings=False,
+                                           write_extrapolation_warnings=False,
+                                           stop_on_extrapolation_warnings=False):
+        self._check(self._L.n2p2b_setup_symmetry_function_statistics(
+            self._h, int(collect_statistics),
+            int(collect_extrapolation_warnings),
+            int(write_extrapolation_warnings),
+            int(stop_on_extrapolation_warnings)))
+
+    def get_num_extrapolation_warnings(self) -> int:
+        return int(self._L.n2p2b_get_num_extrapolation_warnings(self._h))
+
+    def reset_extrapolation_warnings(self):
+        self._check(self._L.n2p2b_reset_extrapolation_warnings(self._h))
+
+    def extrapolation_counts(self):
+        """Warnings per atom of the last evaluation."""
+        out = np.zeros(self.num_atoms, dtype=np.int32)
+        self._check(self._L.n2p2b_get_extrapolation_counts(
+            self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
+        return out
+
     _PRECISIONS = {"fp64": _capi.PRECISION_FP64,
                    "mixed": _capi.PRECISION_MIXED,
                    "bf16": _capi.PRECISION_BF16}
@@ -328,10 +359,14 @@ class Prediction(Mode):
                                                        "weights.%03zu.data")
 
     def setup(self):
+        """Prediction::setup (libnnp/Prediction.cpp:34-46), including its
+        setupSymmetryFunctionStatistics(false, false, true, false): write
+        extrapolation warnings to stderr."""
         self.load_settings_file(self.file_name_settings)
         self.setup_generic()
         self.setup_symmetry_function_scaling(self.file_name_scaling)
         self.setup_neural_network_weights(self.format_weights_files_short)
+        self.setup_symmetry_function_statistics(False, False, True, False)
 
     def predict(self, positions=None, elements=None, box=None):
         """Prediction::predict; with arguments, sets the structure first.

@@ -77,6 +77,11 @@ def _load():
         getattr(L, f).argtypes = [C.c_void_p, _dp, C.c_int]
     L.refh_time_stages.restype = C.c_int
     L.refh_time_stages.argtypes = [C.c_void_p, C.c_int, C.c_int, _dp]
+    L.refh_setup_statistics.restype = C.c_int
+    L.refh_setup_statistics.argtypes = [C.c_void_p] + [C.c_int] * 4
+    L.refh_num_extrapolation_warnings.restype = C.c_long
+    L.refh_num_extrapolation_warnings.argtypes = [C.c_void_p]
+    L.refh_reset_extrapolation_warnings.argtypes = [C.c_void_p]
     _lib = L
     return L
 
@@ -189,6 +194,20 @@ class RefModel:
         out = np.zeros((num_entries, max_slots, 3))
         self.L.refh_dGdr_nbr(self.h, _p(out, _dp), max_slots)
         return out
+
+    def setup_statistics(self, collect_statistics=False, collect_ew=False,
+                         write_ew=False, stop_on_ew=False):
+        """Mode::setupSymmetryFunctionStatistics (Prediction::setup turns
+        on writing extrapolation warnings)."""
+        self.L.refh_setup_statistics(self.h, int(collect_statistics),
+                                     int(collect_ew), int(write_ew),
+                                     int(stop_on_ew))
+
+    def num_extrapolation_warnings(self) -> int:
+        return int(self.L.refh_num_extrapolation_warnings(self.h))
+
+    def reset_extrapolation_warnings(self):
+        self.L.refh_reset_extrapolation_warnings(self.h)
 
     def time_stages(self, threads: int = 0, reps: int = 1):
         t = np.zeros(5)

@@ -416,6 +416,28 @@ int refh_time_stages(void* p, int threads, int reps, double* t_out)
     return 0;
 }
 
+// Mode::setupSymmetryFunctionStatistics (libnnp/Mode.cpp:1103-1137).
+int refh_setup_statistics(void* p, int collect_statistics, int collect_ew,
+                          int write_ew, int stop_on_ew)
+{
+    Handle* h = static_cast<Handle*>(p);
+    h->model.setupSymmetryFunctionStatistics(collect_statistics != 0,
+                                             collect_ew != 0, write_ew != 0,
+                                             stop_on_ew != 0);
+    return 0;
+}
+
+// Mode::getNumExtrapolationWarnings (libnnp/Mode.cpp:2166-2178).
+long refh_num_extrapolation_warnings(void* p)
+{
+    return (long)static_cast<Handle*>(p)->model.getNumExtrapolationWarnings();
+}
+
+void refh_reset_extrapolation_warnings(void* p)
+{
+    static_cast<Handle*>(p)->model.resetExtrapolationWarnings();
+}
+
 int refh_max_threads()
 {
 #ifdef _OPENMP
