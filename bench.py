@@ -348,9 +348,12 @@ def _stage_ms(p, frames_dev, steps):
 
 def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
     """Plain FP64 vs the mixed forms on the same 24,576-atom frames, for the
-    52-SF potential and the wider 92-SF / 64-64-64 softplus potential.
-    Accuracy is measured against the FP64 form on three frames (the FP64
-    form equals the reference to 1e-10, tests/test_gpu_parity.py)."""
+    52-SF potential and the wider 92-SF / 64-64-64 softplus potential, and
+    for the latter the distilled 92-16-1 student (gated by its training
+    range; atoms outside it are re-evaluated by the teacher on the tensor
+    cores).  Accuracy is measured against the FP64 form on three frames (the
+    FP64 form equals the reference to 1e-10, tests/test_gpu_parity.py) and,
+    for the student, also against the mixed-precision teacher."""
     from n2p2_b200.mode import Prediction
     n = len(elem)
     out = {}
@@ -360,9 +363,18 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
         p.setup_symmetry_function_statistics(False, False, False, False)
         p.set_stream(stream.cuda_stream)
         p.set_structure(frames[0], elem, box)
-        ref = None
-        for prec in ("fp64", "mixed", "bf16"):
+        forms = [("fp64", "fp64", None), ("mixed", "mixed", None),
+                 ("bf16", "bf16", None)]
+        sdir = os.path.join(POT_DIR, pot + "_student")
+        if os.path.exists(os.path.join(sdir, "training_range.data")):
+            p.setup_student(sdir)
+            forms += [("student_gated", "mixed", "gated"),
+                      ("student_only", "mixed", "only")]
+        refs = {}
+        for name, prec, smode in forms:
             p.set_precision(prec)
+            if smode is not None:
+                p.set_student_mode(smode)
             p.set_positions(frames[0])
             p.evaluate_nnp(True)
             for s in range(3):
@@ -371,28 +383,37 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
             p.finish()
             t, launches = _time_steps(p, dev_frames, steps, stream, lib)
             stage = _stage_ms(p, dev_frames, min(steps, 10))
-            acc = []
+            acc, gated = [], []
             for s in range(3):
                 p.set_positions(frames[s])
                 p.evaluate_nnp(True)
                 acc.append((p.energy, p.forces().copy()))
+                if smode == "gated":
+                    gated.append(p.student_gated_count() / n)
             entry = {"value": n * steps / t, "unit": "atoms/s",
                      "ms_per_step": 1e3 * t / steps, "steps": steps,
+                     "gpu_launches_per_step": launches / steps,
                      "stage_ms_per_step": dict(zip(STAGES, stage))}
-            if prec == "fp64":
-                ref = acc
-            else:
+            refs[name] = acc
+            for rname in (("fp64", "mixed") if smode else ("fp64",)):
+                if name == rname:
+                    continue
+                ref = refs[rname]
                 de = [(e - e0) / n for (e, _), (e0, _) in zip(acc, ref)]
                 df = np.concatenate([(f - f0).ravel()
                                      for (_, f), (_, f0) in zip(acc, ref)])
-                entry["energy_per_atom_rmse_vs_fp64"] = float(
+                entry[f"energy_per_atom_rmse_vs_{rname}"] = float(
                     np.sqrt(np.mean(np.square(de))))
-                entry["force_rmse_vs_fp64"] = float(
+                entry[f"force_rmse_vs_{rname}"] = float(
                     np.sqrt(np.mean(np.square(df))))
+            if name != "fp64":
                 entry["speedup_vs_fp64"] = (
                     entry["value"] / out[pot]["fp64"]["value"])
-            out.setdefault(pot, {})[prec] = entry
-        out[pot]["force_rms"] = float(np.sqrt(np.mean(np.square(ref[0][1]))))
+            if gated:
+                entry["gated_fraction"] = float(np.mean(gated))
+            out.setdefault(pot, {})[name] = entry
+        out[pot]["force_rms"] = float(
+            np.sqrt(np.mean(np.square(refs["fp64"][0][1]))))
         p.close()
     out["targets"] = {"energy_per_atom_rmse": 1e-4, "force_rmse": 5e-3,
                       "units": "potential energy units; energy / bohr"}
@@ -401,7 +422,11 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
         "mixed": "FP32 symmetry functions + dG/dr; NN on tcgen05 with BF16 "
                  "hi/lo operand pairs (3 MMAs per step), FP32 accumulation; "
                  "FP64 displacements, energy sum, force accumulation",
-        "bf16": "as mixed with single BF16 operands (1 MMA per step)"}
+        "bf16": "as mixed with single BF16 operands (1 MMA per step)",
+        "student_gated": "FP32 symmetry functions; distilled 92-16-1 FP32 "
+                         "student for atoms inside its training range, the "
+                         "mixed-precision teacher for the others",
+        "student_only": "the student for every atom (no gate)"}
     return out
 
 

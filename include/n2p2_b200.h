@@ -190,6 +190,51 @@ int     n2p2b_reset_extrapolation_warnings(n2p2b_context* ctx);
 /* Warnings per atom of the last evaluation (num_atoms ints). */
 int     n2p2b_get_extrapolation_counts(n2p2b_context* ctx, int32_t* counts);
 
+/* ---- distilled student network --------------------------------------- */
+
+/* No counterpart in the reference.  A student is a smaller atomic network
+ * (its own potential directory: input.nn with exactly this potential's
+ * symmetry functions, the same scaling.data, weights.%03zu.data, and
+ * training_range.data once trained) that runs in FP32 on the FP32 symmetry
+ * functions of a mixed precision.  Gated, every atom that has a symmetry
+ * function outside the student's training range (the test of
+ * Element::updateSymmetryFunctionStatistics with that range) is re-evaluated
+ * by this potential's own network on the tensor cores. */
+#define N2P2B_STUDENT_OFF        0  /* the potential's network only        */
+#define N2P2B_STUDENT_GATED      1  /* student, teacher outside its range  */
+#define N2P2B_STUDENT_ONLY       2  /* student for every atom              */
+int n2p2b_setup_student(n2p2b_context* ctx, const char* directory);
+int n2p2b_set_student_mode(n2p2b_context* ctx, int mode);
+/* Atoms the teacher re-evaluated in the last gated evaluation. */
+int n2p2b_get_student_gated_count(n2p2b_context* ctx, int64_t* count);
+/* One Adam step (hand-written kernels) on a batch of the current structure:
+ * loss = w_energy / B sum (E_i - E_i^label)^2
+ *      + w_force / (3B) sum |F_i - F_i^label|^2 over the batch atoms.
+ * Symmetry functions with derivatives must be current
+ * (n2p2b_calculate_symmetry_function_groups).  energy_labels (num_atoms,
+ * the units of n2p2b_get_atomic_energies), force_labels (num_atoms x 3, the
+ * units of n2p2b_get_forces) and batch
+ * (batch_size atom indices) are device arrays.  loss (host, 2 doubles: the
+ * energy and force terms, or NULL) synchronizes.  Training needs one hidden
+ * tanh layer and a linear output. */
+int n2p2b_student_train_step(n2p2b_context* ctx, const double* energy_labels,
+                             const double* force_labels, const int32_t* batch,
+                             int batch_size, double w_energy, double w_force,
+                             double learning_rate, double* loss);
+int n2p2b_student_reset_optimizer(n2p2b_context* ctx);
+/* The student's FP32 parameter blob as doubles (per element and layer: W
+ * out x in, W^T, b; `size` receives its length).  which = 0: the weights
+ * (get and/or set; W and W^T must be set consistently); which = 1: the
+ * gradient summed in the last training step (get only; the W^T and
+ * unused positions are 0). */
+int n2p2b_student_weights(n2p2b_context* ctx, double* get, const double* set,
+                          int64_t* size, int which);
+/* reset = 1 empties the training range; reset = 0 widens it to cover the
+ * current structure's symmetry functions. */
+int n2p2b_student_update_range(n2p2b_context* ctx, int reset);
+/* Writes weights.%03zu.data and training_range.data into `directory`. */
+int n2p2b_student_write(n2p2b_context* ctx, const char* directory);
+
 /* ---- results ---------------------------------------------------------- */
 
 /* Structure::energy after Prediction::predict (physical units, offsets). */

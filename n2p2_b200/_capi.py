@@ -26,6 +26,9 @@ REMAP = 1
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 PRECISION_BF16 = 2
+STUDENT_OFF = 0
+STUDENT_GATED = 1
+STUDENT_ONLY = 2
 
 _dp = C.POINTER(C.c_double)
 _i32p = C.POINTER(C.c_int32)
@@ -45,6 +48,16 @@ SIGNATURES = {
     "n2p2b_get_num_extrapolation_warnings": (C.c_int64, [_vp]),
     "n2p2b_reset_extrapolation_warnings": (C.c_int, [_vp]),
     "n2p2b_get_extrapolation_counts": (C.c_int, [_vp, _i32p]),
+    "n2p2b_setup_student": (C.c_int, [_vp, C.c_char_p]),
+    "n2p2b_set_student_mode": (C.c_int, [_vp, C.c_int]),
+    "n2p2b_get_student_gated_count": (C.c_int, [_vp, _i64p]),
+    "n2p2b_student_train_step": (C.c_int, [
+        _vp, _vp, _vp, _vp, C.c_int, C.c_double, C.c_double, C.c_double,
+        _dp]),
+    "n2p2b_student_reset_optimizer": (C.c_int, [_vp]),
+    "n2p2b_student_weights": (C.c_int, [_vp, _dp, _dp, _i64p, C.c_int]),
+    "n2p2b_student_update_range": (C.c_int, [_vp, C.c_int]),
+    "n2p2b_student_write": (C.c_int, [_vp, C.c_char_p]),
     "n2p2b_load_settings_file": (C.c_int, [_vp, C.c_char_p]),
     "n2p2b_setup_generic": (C.c_int, [_vp]),
     "n2p2b_setup_symmetry_function_scaling": (C.c_int, [_vp, C.c_char_p]),

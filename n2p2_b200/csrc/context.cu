@@ -15,7 +15,9 @@
 #include <cstdio>
 #include <cstring>
 #include <exception>
+#include <fstream>
 #include <numeric>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -200,7 +202,6 @@ struct n2p2b_context
     bool         tcOk[2] = {false, false};
     std::string  tcWhy[2];
     DevBuf       tcW[2], tcF[2];
-    int          tileBeg[kMaxElem + 1] = {};
     int          tcGrid[2] = {0, 0};
     // Extrapolation warnings (Mode::setupSymmetryFunctionStatistics).
     bool         ewCheck = false, ewWrite = false, ewStop = false;
@@ -209,6 +210,24 @@ struct n2p2b_context
     std::vector<Range> ewRangeHost;
     std::vector<SFScale> sfScaleHost;
     DevBuf       ewRange, ewPerAtom;
+
+    // Distilled student network (FP32, same symmetry functions).
+    struct Student
+    {
+        bool               loaded = false;
+        Potential          pot;
+        NNParams           nnp{};
+        std::vector<float> blob;
+        int                mode = 0;         // 0 off, 1 gated, 2 student only
+        bool               trainable = false;
+        std::string        whyNot;
+        std::vector<Range> range;            // training range (unscaled)
+        bool               haveRange = false;
+        long               step = 0;         // Adam steps taken
+        int                maxH = 0, maxNin = 0, maxParams = 0;
+        DevBuf             w, m, v, grad, gpart, rE, rF, u, loss, dRange,
+                           list, listCount;
+    } stu;
 
     // Structure.
     long         n = 0;
@@ -307,6 +326,11 @@ struct n2p2b_context
             for (auto& e : se.ev) cudaEventDestroy(e);
         for (auto& se : freeEvents)
             for (auto& e : se.ev) cudaEventDestroy(e);
+        for (DevBuf* b : {&stu.w, &stu.m, &stu.v, &stu.grad, &stu.gpart,
+                          &stu.rE,
+                          &stu.rF, &stu.u, &stu.loss, &stu.dRange, &stu.list,
+                          &stu.listCount})
+            b->release();
         for (DevBuf* b : {&sfScale, &nnW, &slotSF, &tcW[0], &tcF[0], &tcW[1],
                           &tcF[1], &ewRange, &ewPerAtom, &posIn, &pos, &elem,
                           &atomsByElem, &cellOf, &cellCount, &cellFill,
@@ -360,6 +384,47 @@ struct n2p2b_context
             }
         }
         return (int)ns;
+    }
+
+    // Device layout of a potential's networks: per element and layer W
+    // (out x in, row-major), W^T and b in one blob (NNParams offsets).
+    static void nnBlob(Potential const& pt, NNParams& P,
+                       std::vector<double>& blob)
+    {
+        int const ne = pt.numElements();
+        std::memset(&P, 0, sizeof(P));
+        P.numElements = ne;
+        blob.clear();
+        int maxW = 1;
+        for (int e = 0; e < ne; ++e)
+        {
+            NeuralNet const& nn = pt.elements[e].nn;
+            if (nn.numLayers > kMaxLayers)
+                throw std::runtime_error("ERROR: Too many NN layers.\n");
+            P.numLayers[e] = nn.numLayers;
+            P.normalizeNeurons = nn.normalizeNeurons ? 1 : 0;
+            for (int l = 0; l < nn.numLayers; ++l)
+            {
+                P.width[e][l] = nn.neurons[l];
+                P.act[e][l] = nn.activations[l];
+                maxW = std::max(maxW, nn.neurons[l]);
+            }
+            for (int l = 1; l < nn.numLayers; ++l)
+            {
+                int const ni = nn.neurons[l - 1], no = nn.neurons[l];
+                P.woff[e][l] = (long)blob.size();
+                blob.insert(blob.end(), nn.W[l].begin(), nn.W[l].end());
+                P.wtoff[e][l] = (long)blob.size();
+                for (int j = 0; j < ni; ++j)
+                    for (int o = 0; o < no; ++o)
+                        blob.push_back(nn.W[l][(std::size_t)o * ni + j]);
+                P.boff[e][l] = (long)blob.size();
+                blob.insert(blob.end(), nn.b[l].begin(), nn.b[l].end());
+            }
+        }
+        if (maxW > kMaxWidth)
+            throw std::runtime_error("ERROR: NN layer wider than supported.\n");
+        P.maxWidth = maxW;
     }
 
     void buildTables()
@@ -483,39 +548,8 @@ struct n2p2b_context
         sfp.groupBeg[ne] = gi;
 
         // NN blob.
-        std::memset(&nnp, 0, sizeof(nnp));
-        nnp.numElements = ne;
         std::vector<double> blob;
-        int maxW = 1;
-        for (int e = 0; e < ne; ++e)
-        {
-            NeuralNet const& nn = pot.elements[e].nn;
-            if (nn.numLayers > kMaxLayers)
-                throw std::runtime_error("ERROR: Too many NN layers.\n");
-            nnp.numLayers[e] = nn.numLayers;
-            nnp.normalizeNeurons = nn.normalizeNeurons ? 1 : 0;
-            for (int l = 0; l < nn.numLayers; ++l)
-            {
-                nnp.width[e][l] = nn.neurons[l];
-                nnp.act[e][l] = nn.activations[l];
-                maxW = std::max(maxW, nn.neurons[l]);
-            }
-            for (int l = 1; l < nn.numLayers; ++l)
-            {
-                int const ni = nn.neurons[l - 1], no = nn.neurons[l];
-                nnp.woff[e][l] = (long)blob.size();
-                blob.insert(blob.end(), nn.W[l].begin(), nn.W[l].end());
-                nnp.wtoff[e][l] = (long)blob.size();
-                for (int j = 0; j < ni; ++j)
-                    for (int o = 0; o < no; ++o)
-                        blob.push_back(nn.W[l][(std::size_t)o * ni + j]);
-                nnp.boff[e][l] = (long)blob.size();
-                blob.insert(blob.end(), nn.b[l].begin(), nn.b[l].end());
-            }
-        }
-        if (maxW > kMaxWidth)
-            throw std::runtime_error("ERROR: NN layer wider than supported.\n");
-        nnp.maxWidth = maxW;
+        nnBlob(pot, nnp, blob);
         std::vector<unsigned char> tcWeights[2];
         std::vector<float> tcFloats[2];
         for (int k = 0; k < 2; ++k)
@@ -568,6 +602,12 @@ struct n2p2b_context
     void requireStructure() const
     {
         if (n <= 0) throw StateError("ERROR: No structure set.\n");
+    }
+
+    // The network changed: symmetry functions and neighbor list stand.
+    void invalidateNN()
+    {
+        haveNN = haveNNDeriv = haveE = haveF = false;
     }
 
     void invalidate()
@@ -667,14 +707,6 @@ struct n2p2b_context
         }
         es.start[ne] = (int)byElem.size();
         for (int e = ne + 1; e <= kMaxElem; ++e) es.start[e] = es.start[ne];
-        // Tensor-core tiles: 128 atoms of one element each.
-        std::memset(tileBeg, 0, sizeof(tileBeg));
-        for (int e = 0; e < ne; ++e)
-        {
-            int const cnt = es.start[e + 1] - es.start[e];
-            tileBeg[e + 1] = tileBeg[e] + (cnt + kTcRows - 1) / kTcRows;
-        }
-        for (int e = ne + 1; e <= kMaxElem; ++e) tileBeg[e] = tileBeg[ne];
 
         posIn.ensure(sizeof(double) * 3 * n);
         pos.ensure(sizeof(double) * 3 * n);
@@ -717,6 +749,7 @@ struct n2p2b_context
         dGdrSelf.ensure(realBytes() * n * maxSF * 3);
         Ei.ensure(sizeof(double) * n);
         ewPerAtom.ensure(sizeof(int) * n);
+        if (stu.loaded) stu.list.ensure(sizeof(int) * n);
         selfF.ensure(sizeof(double) * n * 3);
         F.ensure(sizeof(double) * n * 3);
         energyOut.ensure(sizeof(double) * 2);
@@ -961,8 +994,441 @@ struct n2p2b_context
         return first;
     }
 
+    // ---- distilled student ------------------------------------------------
+
+    static bool sameSF(SymFnc const& a, SymFnc const& b)
+    {
+        return a.type == b.type && a.ec == b.ec && a.e1 == b.e1
+            && a.e2 == b.e2 && a.eta == b.eta && a.rs == b.rs && a.rc == b.rc
+            && a.zeta == b.zeta && a.lambda == b.lambda
+            && a.cutoffType == b.cutoffType && a.cutoffAlpha == b.cutoffAlpha
+            && a.scalingType == b.scalingType && a.Smin == b.Smin
+            && a.Smax == b.Smax && a.Gmin == b.Gmin && a.Gmax == b.Gmax
+            && a.Gmean == b.Gmean && a.Gsigma == b.Gsigma;
+    }
+
+    // Loads a student potential directory: input.nn with this potential's
+    // symmetry functions, its scaling.data, the student's
+    // weights.%03zu.data and (once trained) training_range.data.
+    void setupStudent(std::string d)
+    {
+        requireReady();
+        if (!d.empty() && d.back() != '/') d += "/";
+        Student s;
+        s.pot.loadSettingsFile(d + "input.nn");
+        s.pot.setupGeneric();
+        s.pot.setupSymmetryFunctionScaling(d + "scaling.data");
+        s.pot.setupNeuralNetworkWeights(d + "weights.%03zu.data");
+        int const ne = pot.numElements();
+        if (s.pot.numElements() != ne)
+            throw std::runtime_error("ERROR: The student has other elements "
+                                     "than the potential.\n");
+        for (int e = 0; e < ne; ++e)
+        {
+            Element const& a = pot.elements[e];
+            Element const& b = s.pot.elements[e];
+            if (a.symbol != b.symbol || a.sfs.size() != b.sfs.size())
+                throw std::runtime_error("ERROR: The student's elements or "
+                                         "symmetry functions differ from the "
+                                         "potential's.\n");
+            for (std::size_t k = 0; k < a.sfs.size(); ++k)
+                if (!sameSF(a.sfs[k], b.sfs[k]))
+                    throw std::runtime_error(
+                        "ERROR: The student's symmetry functions or scaling "
+                        "differ from the potential's.\n");
+        }
+        std::vector<double> bd;
+        nnBlob(s.pot, s.nnp, bd);
+        s.blob.assign(bd.begin(), bd.end());
+        s.trainable = true;
+        for (int e = 0; e < ne; ++e)
+        {
+            NNParams const& q = s.nnp;
+            bool const ok = q.numLayers[e] == 3 && q.act[e][1] == AF_TANH
+                         && q.act[e][2] == AF_IDENTITY && q.width[e][2] == 1
+                         && !q.normalizeNeurons && q.width[e][1] <= 64;
+            if (!ok)
+            {
+                s.trainable = false;
+                s.whyNot = "training needs one hidden tanh layer (<= 64 "
+                           "neurons), a linear single output and no "
+                           "normalize_nodes";
+            }
+            s.maxH = std::max(s.maxH, q.width[e][1]);
+            s.maxNin = std::max(s.maxNin, q.width[e][0]);
+            s.maxParams = std::max(s.maxParams, q.width[e][1] * q.width[e][0]
+                                                + 2 * q.width[e][1] + 1);
+        }
+        s.range.assign((std::size_t)ne * maxSF, Range{DBL_MAX, -DBL_MAX});
+        std::ifstream rf(d + "training_range.data");
+        if (rf.is_open())
+        {
+            std::string line;
+            while (std::getline(rf, line))
+            {
+                if (line.empty() || line[0] == '#') continue;
+                std::istringstream is(line);
+                int e = 0, k = 0;
+                double lo = 0.0, hi = 0.0;
+                if (!(is >> e >> k >> lo >> hi)) continue;
+                if (e < 1 || e > ne || k < 1 || k > maxSF)
+                    throw std::runtime_error("ERROR: Bad training_range.data "
+                                             "line.\n");
+                s.range[(std::size_t)(e - 1) * maxSF + (k - 1)] =
+                    Range{lo, hi};
+            }
+            s.haveRange = true;
+        }
+        s.loaded = true;
+        // Keep the device buffers of a previous student (grow-only).
+        std::swap(s.w, stu.w);
+        std::swap(s.m, stu.m);
+        std::swap(s.v, stu.v);
+        std::swap(s.grad, stu.grad);
+        std::swap(s.gpart, stu.gpart);
+        std::swap(s.rE, stu.rE);
+        std::swap(s.rF, stu.rF);
+        std::swap(s.u, stu.u);
+        std::swap(s.loss, stu.loss);
+        std::swap(s.dRange, stu.dRange);
+        std::swap(s.list, stu.list);
+        std::swap(s.listCount, stu.listCount);
+        stu = std::move(s);
+        if (hostOnly()) return;
+        activate();
+        stu.w.ensure(sizeof(float) * stu.blob.size());
+        ck(cudaMemcpy(stu.w.p, stu.blob.data(), sizeof(float) * stu.blob.size(),
+                      cudaMemcpyHostToDevice), "copy student weights");
+        resetOptimizer();
+        stu.dRange.ensure(sizeof(Range) * stu.range.size());
+        ck(cudaMemcpy(stu.dRange.p, stu.range.data(),
+                      sizeof(Range) * stu.range.size(),
+                      cudaMemcpyHostToDevice), "copy training range");
+        stu.listCount.ensure(sizeof(int) * kMaxElem);
+        stu.loss.ensure(sizeof(double) * 2);
+        if (n > 0) stu.list.ensure(sizeof(int) * n);
+        invalidate();
+    }
+
+    void resetOptimizer()
+    {
+        stu.m.ensure(sizeof(float) * stu.blob.size());
+        stu.v.ensure(sizeof(float) * stu.blob.size());
+        stu.grad.ensure(sizeof(float) * stu.blob.size());
+        ck(cudaMemsetAsync(stu.grad.p, 0, sizeof(float) * stu.blob.size(),
+                           stream), "clear gradient");
+        ck(cudaMemsetAsync(stu.m.p, 0, sizeof(float) * stu.blob.size(), stream),
+           "clear Adam state");
+        ck(cudaMemsetAsync(stu.v.p, 0, sizeof(float) * stu.blob.size(), stream),
+           "clear Adam state");
+        stu.step = 0;
+    }
+
+    void requireStudent(bool train) const
+    {
+        if (!stu.loaded)
+            throw StateError("ERROR: No student network set up.\n");
+        if (train && !stu.trainable)
+            throw std::runtime_error("ERROR: The student cannot be trained: "
+                                     + stu.whyNot + ".\n");
+        if (precision == PREC_FP64)
+            throw StateError("ERROR: The student runs on FP32 symmetry "
+                             "functions: select a mixed precision first.\n");
+    }
+
+    void setStudentMode(int mode)
+    {
+        if (mode < 0 || mode > 2)
+            throw std::invalid_argument("ERROR: Unknown student mode.\n");
+        if (mode != 0)
+        {
+            requireStudent(false);
+            if (mode == 1 && !stu.haveRange)
+                throw StateError("ERROR: The gated student needs its "
+                                 "training range.\n");
+            if (mode == 1 && !tcOk[precision == PREC_MIXED ? 1 : 0])
+                throw std::runtime_error("ERROR: The gated student needs the "
+                                         "tensor-core form of the potential: "
+                                         + tcWhy[precision == PREC_MIXED]
+                                         + ".\n");
+        }
+        stu.mode = mode;
+        invalidateNN();
+    }
+
+    void enqueueStudentNN(bool deriv)
+    {
+        NNLaunch L;
+        L.n = (int)n;
+        L.derivatives = deriv ? 1 : 0;
+        L.maxSF = maxSF;
+        L.precision = PREC_MIXED;
+        L.elem = elem.as<int>();
+        L.weights = stu.w.p;
+        L.G = G.p;
+        L.energy = Ei.as<double>();
+        L.dEdG = dEdG.p;
+        L.status = status.as<int>();
+        launchNeuralNetworks(stu.nnp, L, stream);
+    }
+
+    // Student for every atom; atoms with any symmetry function outside the
+    // student's training range are re-evaluated by the potential's own
+    // network on the tensor cores.
+    void enqueueGatedStudent(bool deriv)
+    {
+        enqueueStudentNN(deriv);
+        if (stu.mode != 1) return;
+        int const k = (precision == PREC_MIXED) ? 1 : 0;
+        ck(cudaMemsetAsync(stu.listCount.p, 0, sizeof(int) * kMaxElem, stream),
+           "clear gate lists");
+        EWLaunch E;
+        E.n = (int)n;
+        E.maxSF = maxSF;
+        E.precision = precision;
+        for (int e = 0; e < pot.numElements(); ++e)
+        {
+            E.numSF[e] = sfp.numSF[e];
+            E.listStart[e] = es.start[e];
+        }
+        E.elem = elem.as<int>();
+        E.G = G.p;
+        E.scale = sfScale.as<SFScale>();
+        E.range = stu.dRange.as<Range>();
+        E.list = stu.list.as<int>();
+        E.listCount = stu.listCount.as<int>();
+        E.status = status.as<int>();
+        E.countSlot = ST_GATE_COUNT;
+        launchExtrapolationCheck(E, stream);
+        if (tcGrid[k] == 0)
+        {
+            ck(cudaDeviceGetAttribute(&smCount, cudaDevAttrMultiProcessorCount,
+                                      device), "device attribute");
+            tcGrid[k] = smCount * tcBlocksPerSM(tcp[k]);
+        }
+        TcNNLaunch T;
+        T.n = (int)n;
+        T.derivatives = deriv ? 1 : 0;
+        T.maxSF = maxSF;
+        T.atomsByElem = stu.list.as<int>();
+        T.es = es;
+        T.listCount = stu.listCount.as<int>();
+        T.grid = tcGrid[k];
+        T.wblob = tcW[k].as<unsigned char>();
+        T.fblob = tcF[k].as<float>();
+        T.G = G.as<float>();
+        T.energy = Ei.as<double>();
+        T.dEdG = dEdG.as<float>();
+        T.status = status.as<int>();
+        launchNeuralNetworksTC(tcp[k], T, stream);
+    }
+
+    long gatedCount()
+    {
+        requireStudent(false);
+        if (stu.mode != 1) return 0;
+        int c[kMaxElem] = {};
+        ck(cudaMemcpy(c, stu.listCount.p, sizeof(int) * kMaxElem,
+                      cudaMemcpyDeviceToHost), "read gate counts");
+        long t = 0;
+        for (int e = 0; e < pot.numElements(); ++e) t += c[e];
+        return t;
+    }
+
+    // One Adam step of the student on a batch of the current structure's
+    // atoms (symmetry functions and derivatives must be current).
+    void studentTrainStep(double const* labelE, double const* labelF,
+                          int const* batch, int batchSize, double wE,
+                          double wF, double lr, double* lossOut)
+    {
+        requireStudent(true);
+        if (!haveSF || !haveSFDeriv)
+            throw StateError("ERROR: Calculate the symmetry functions with "
+                             "derivatives first.\n");
+        if (batchSize <= 0 || !labelE || !labelF || !batch)
+            throw std::invalid_argument("ERROR: Bad training batch.\n");
+        activate();
+        enqueueStudentNN(true);
+        enqueueForces();
+        stu.rE.ensure(sizeof(float) * n);
+        stu.rF.ensure(sizeof(float) * n * 3);
+        stu.u.ensure(sizeof(float) * n * maxSF);
+        ck(cudaMemsetAsync(stu.rE.p, 0, sizeof(float) * n, stream), "memset");
+        ck(cudaMemsetAsync(stu.rF.p, 0, sizeof(float) * n * 3, stream),
+           "memset");
+        ck(cudaMemsetAsync(stu.loss.p, 0, sizeof(double) * 2, stream),
+           "memset");
+        StudentLaunch S;
+        int const ne = pot.numElements();
+        S.n = (int)n;
+        S.maxSF = maxSF;
+        S.maxSlots = maxSlots;
+        S.numElements = ne;
+        S.precision = precision;
+        for (int e = 0; e < ne; ++e)
+        {
+            S.numSF[e] = sfp.numSF[e];
+            for (int f = 0; f < ne; ++f) S.numSlots[e][f] = sfp.numSlots[e][f];
+            S.hidden[e] = stu.nnp.width[e][1];
+            S.woff1[e] = stu.nnp.woff[e][1];
+            S.wtoff1[e] = stu.nnp.wtoff[e][1];
+            S.boff1[e] = stu.nnp.boff[e][1];
+            S.woff2[e] = stu.nnp.woff[e][2];
+            S.wtoff2[e] = stu.nnp.wtoff[e][2];
+            S.boff2[e] = stu.nnp.boff[e][2];
+        }
+        S.elem = elem.as<int>();
+        S.nbrOff = nbrOff.as<int>();
+        S.nbrIdx = nbrIdx.as<int>();
+        S.nbrCountElem = nbrCountElem.as<int>();
+        S.slotSF = slotSF.as<int16_t>();
+        S.atomsByElem = atomsByElem.as<int>();
+        S.es = es;
+        int const blocks = studentGradBlocks(es, ne, S.blkBeg);
+        S.paramStride = stu.maxParams;
+        stu.gpart.ensure(sizeof(float) * std::max(blocks, 1)
+                         * (std::size_t)stu.maxParams);
+        S.G = G.p;
+        S.dGdrSelf = dGdrSelf.p;
+        S.dGdr = dGdr.p;
+        S.Ei = Ei.as<double>();
+        S.F = F.as<double>();
+        S.labelE = labelE;
+        S.labelF = labelF;
+        S.batch = batch;
+        S.batchSize = batchSize;
+        S.wE = wE;
+        S.wF = wF;
+        S.eScale = pot.normalize ? 1.0 / pot.convEnergy : 1.0;
+        S.fScale = pot.normalize ? pot.convLength / pot.convEnergy : 1.0;
+        S.rE = stu.rE.as<float>();
+        S.rF = stu.rF.as<float>();
+        S.u = stu.u.as<float>();
+        S.blob = stu.w.as<float>();
+        S.m = stu.m.as<float>();
+        S.v = stu.v.as<float>();
+        S.gpart = stu.gpart.as<float>();
+        S.grad = stu.grad.as<float>();
+        S.loss = stu.loss.as<double>();
+        S.lr = (float)lr;
+        ++stu.step;
+        S.bc1 = (float)(1.0 - std::pow((double)S.beta1, (double)stu.step));
+        S.bc2 = (float)(1.0 - std::pow((double)S.beta2, (double)stu.step));
+        launchStudentTrainStep(S, studentGradSmem(stu.maxNin, stu.maxH),
+                               stu.maxParams, stream);
+        checkLaunch("student training step");
+        haveNN = haveNNDeriv = haveE = haveF = false;
+        if (lossOut)
+        {
+            double l[2];
+            ck(cudaMemcpyAsync(l, stu.loss.p, sizeof(l), cudaMemcpyDeviceToHost,
+                               stream), "read loss");
+            ck(cudaStreamSynchronize(stream), "synchronize");
+            lossOut[0] = wE * l[0] / batchSize;
+            lossOut[1] = wF * l[1] / (3.0 * batchSize);
+        }
+    }
+
+    void studentRange(bool reset)
+    {
+        requireStudent(false);
+        activate();
+        if (reset)
+        {
+            std::fill(stu.range.begin(), stu.range.end(),
+                      Range{DBL_MAX, -DBL_MAX});
+            ck(cudaMemcpy(stu.dRange.p, stu.range.data(),
+                          sizeof(Range) * stu.range.size(),
+                          cudaMemcpyHostToDevice), "reset range");
+            stu.haveRange = false;
+            return;
+        }
+        if (!haveSF)
+            throw StateError("ERROR: Calculate the symmetry functions "
+                             "first.\n");
+        RangeLaunch R;
+        int const ne = pot.numElements();
+        R.maxSF = maxSF;
+        R.numElements = ne;
+        R.precision = precision;
+        for (int e = 0; e < ne; ++e) R.numSF[e] = sfp.numSF[e];
+        R.atomsByElem = atomsByElem.as<int>();
+        R.es = es;
+        R.blkBeg[0] = 0;
+        for (int e = 0; e < ne; ++e)
+            R.blkBeg[e + 1] = R.blkBeg[e]
+                            + (es.start[e + 1] - es.start[e] + 255) / 256;
+        for (int e = ne + 1; e <= kMaxElem; ++e) R.blkBeg[e] = R.blkBeg[ne];
+        R.G = G.p;
+        R.scale = sfScale.as<SFScale>();
+        R.range = stu.dRange.as<Range>();
+        launchStudentRange(R, stream);
+        checkLaunch("training range");
+        stu.haveRange = true;
+    }
+
+    // Writes the student's weights (n2p2 weights.%03zu.data, the order of
+    // NeuralNetwork::setConnections) and its training range.
+    void writeStudent(std::string d)
+    {
+        requireStudent(false);
+        if (!d.empty() && d.back() != '/') d += "/";
+        activate();
+        ck(cudaStreamSynchronize(stream), "synchronize");
+        std::vector<float> b(stu.blob.size());
+        ck(cudaMemcpy(b.data(), stu.w.p, sizeof(float) * b.size(),
+                      cudaMemcpyDeviceToHost), "read student weights");
+        ck(cudaMemcpy(stu.range.data(), stu.dRange.p,
+                      sizeof(Range) * stu.range.size(),
+                      cudaMemcpyDeviceToHost), "read range");
+        NNParams const& q = stu.nnp;
+        for (int e = 0; e < pot.numElements(); ++e)
+        {
+            char name[64];
+            std::snprintf(name, sizeof(name), "weights.%03d.data",
+                          stu.pot.elements[e].atomicNumber);
+            std::FILE* f = std::fopen((d + name).c_str(), "w");
+            if (!f)
+                throw std::runtime_error("ERROR: Cannot write " + d + name
+                                         + ".\n");
+            std::fprintf(f, "# student weights of element %s (order of "
+                            "NeuralNetwork::setConnections)\n",
+                         stu.pot.elements[e].symbol.c_str());
+            for (int l = 1; l < q.numLayers[e]; ++l)
+            {
+                int const ni = q.width[e][l - 1], no = q.width[e][l];
+                for (int j = 0; j < ni; ++j)
+                    for (int k = 0; k < no; ++k)
+                        std::fprintf(f, "%24.16E\n",
+                                     (double)b[q.woff[e][l] + (long)k * ni + j]);
+                for (int k = 0; k < no; ++k)
+                    std::fprintf(f, "%24.16E\n", (double)b[q.boff[e][l] + k]);
+            }
+            std::fclose(f);
+        }
+        std::FILE* f = std::fopen((d + "training_range.data").c_str(), "w");
+        if (!f)
+            throw std::runtime_error("ERROR: Cannot write "
+                                     + d + "training_range.data.\n");
+        std::fprintf(f, "# element SF min max of the unscaled symmetry "
+                        "functions over the student's training data\n");
+        for (int e = 0; e < pot.numElements(); ++e)
+            for (int k = 0; k < sfp.numSF[e]; ++k)
+            {
+                Range const& r = stu.range[(std::size_t)e * maxSF + k];
+                std::fprintf(f, "%d %d %24.16E %24.16E\n", e + 1, k + 1, r.lo,
+                             r.hi);
+            }
+        std::fclose(f);
+    }
+
     void enqueueNN(bool deriv)
     {
+        if (stu.mode != 0)
+        {
+            enqueueGatedStudent(deriv);
+            return;
+        }
         if (precision != PREC_FP64)
         {
             int const k = (precision == PREC_MIXED) ? 1 : 0;
@@ -983,7 +1449,6 @@ struct n2p2b_context
             T.maxSF = maxSF;
             T.atomsByElem = atomsByElem.as<int>();
             T.es = es;
-            std::memcpy(T.tileBeg, tileBeg, sizeof(tileBeg));
             T.grid = tcGrid[k];
             T.wblob = tcW[k].as<unsigned char>();
             T.fblob = tcF[k].as<float>();
@@ -1389,6 +1854,93 @@ int n2p2b_set_precision(n2p2b_context* ctx, int mode)
 int n2p2b_get_precision(n2p2b_context const* ctx)
 {
     return ctx ? ctx->precision : N2P2B_ERR_ARGUMENT;
+}
+
+int n2p2b_setup_student(n2p2b_context* ctx, char const* directory)
+{
+    return guarded(ctx, [&] {
+        if (!directory) throw std::invalid_argument("ERROR: directory");
+        ctx->setupStudent(directory);
+    });
+}
+
+int n2p2b_set_student_mode(n2p2b_context* ctx, int mode)
+{
+    return guarded(ctx, [&] { ctx->setStudentMode(mode); });
+}
+
+int n2p2b_get_student_gated_count(n2p2b_context* ctx, int64_t* count)
+{
+    return guarded(ctx, [&] {
+        if (!count) throw std::invalid_argument("ERROR: count");
+        ctx->activate();
+        *count = ctx->gatedCount();
+    });
+}
+
+int n2p2b_student_train_step(n2p2b_context* ctx, double const* energy_labels,
+                             double const* force_labels, int32_t const* batch,
+                             int batch_size, double w_energy, double w_force,
+                             double learning_rate, double* loss)
+{
+    return guarded(ctx, [&] {
+        ctx->studentTrainStep(energy_labels, force_labels, batch, batch_size,
+                              w_energy, w_force, learning_rate, loss);
+    });
+}
+
+int n2p2b_student_weights(n2p2b_context* ctx, double* get,
+                          double const* set, int64_t* size, int which)
+{
+    return guarded(ctx, [&] {
+        ctx->requireStudent(false);
+        ctx->activate();
+        std::size_t const m = ctx->stu.blob.size();
+        if (size) *size = (int64_t)m;
+        DevBuf& b = (which == 1) ? ctx->stu.grad : ctx->stu.w;
+        if (which != 0 && which != 1)
+            throw std::invalid_argument("ERROR: which");
+        std::vector<float> f(m);
+        if (get)
+        {
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            ck(cudaMemcpy(f.data(), b.p, sizeof(float) * m,
+                          cudaMemcpyDeviceToHost), "read student weights");
+            for (std::size_t k = 0; k < m; ++k) get[k] = f[k];
+        }
+        if (set)
+        {
+            if (which != 0)
+                throw std::invalid_argument("ERROR: only weights are set");
+            for (std::size_t k = 0; k < m; ++k) f[k] = (float)set[k];
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            ck(cudaMemcpy(b.p, f.data(), sizeof(float) * m,
+                          cudaMemcpyHostToDevice), "write student weights");
+            ctx->invalidateNN();
+        }
+    });
+}
+
+int n2p2b_student_reset_optimizer(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] {
+        ctx->requireStudent(false);
+        ctx->activate();
+        ctx->resetOptimizer();
+    });
+}
+
+int n2p2b_student_update_range(n2p2b_context* ctx, int reset)
+{
+    return guarded(ctx, [&] { ctx->studentRange(reset != 0); });
+}
+
+int n2p2b_student_write(n2p2b_context* ctx, char const* directory)
+{
+    return guarded(ctx, [&] {
+        if (!directory) throw std::invalid_argument("ERROR: directory");
+        ctx->writeStudent(directory);
+    });
 }
 
 int n2p2b_setup_symmetry_function_statistics(n2p2b_context* ctx,

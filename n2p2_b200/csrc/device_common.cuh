@@ -16,7 +16,8 @@ enum StatusIndex
     ST_TOTAL_NBR = 1,   // total neighbor entries of the last list
     ST_MAX_NBR = 2,     // largest per-atom neighbor count
     ST_BAD_ATOM = 3,    // first atom that raised an error flag (or -1)
-    ST_EW_COUNT = 4,    // extrapolation-warning count (gate)
+    ST_EW_COUNT = 4,    // extrapolation-warning count
+    ST_GATE_COUNT = 5,  // symmetry functions outside the student's range
     ST_NUM = 8
 };
 

@@ -110,17 +110,19 @@ int sfAtomsPerBlock();
 // 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
 int sfDefaultVariant(SFParams const& P);
 
-// Atomic neural networks (forward + dE/dG), FP64.
+// Atomic neural networks (forward + dE/dG) on the SIMT cores: FP64 (plain
+// form) or FP32 (precision != PREC_FP64: the distilled student network).
 struct NNLaunch
 {
     int           n = 0;
     int           derivatives = 1;
     int           maxSF = 0;
+    int           precision = PREC_FP64;  // type of weights, G and dE/dG
     int const*    elem = nullptr;
-    double const* weights = nullptr;  // blob, offsets in NNParams
-    double const* G = nullptr;
+    void const*   weights = nullptr;  // blob, offsets in NNParams
+    void const*   G = nullptr;
     double*       energy = nullptr;   // [n]
-    double*       dEdG = nullptr;     // [n][maxSF]
+    void*         dEdG = nullptr;     // [n][maxSF]
     int const*    status = nullptr;
 };
 
@@ -180,9 +182,12 @@ struct TcNNLaunch
     int                n = 0;
     int                derivatives = 1;
     int                maxSF = 0;
+    // Atoms of element e: atomsByElem[es.start[e] + k] for k < count_e, with
+    // count_e = es.start[e + 1] - es.start[e], or listCount[e] (device) when
+    // listCount is set (the teacher re-evaluating gated atoms).
     int const*         atomsByElem = nullptr;
     ElemStarts         es{};
-    int                tileBeg[kMaxElem + 1] = {};  // first tile per element
+    int const*         listCount = nullptr;
     int                grid = 0;
     unsigned char const* wblob = nullptr;  // BF16 weights (UMMA layout)
     float const*       fblob = nullptr;    // FP32 biases, output weights
@@ -223,10 +228,83 @@ struct EWLaunch
     int*           list = nullptr;          // atoms with warnings, per
     int*           listCount = nullptr;     // element at listStart[e]
     int            listStart[kMaxElem] = {};
-    int*           status = nullptr;        // ST_EW_COUNT accumulates
+    int*           status = nullptr;
+    int            countSlot = ST_EW_COUNT;  // status word that accumulates
 };
 
 void launchExtrapolationCheck(EWLaunch const& L, cudaStream_t s);
+
+// Student training (kernels_student.cu).  The student network of element e
+// has one hidden layer of hidden[e] tanh neurons and a linear output; its
+// FP32 weights live in `blob` at the NNParams-style offsets below (W1 out x
+// in, W1^T, b1, W2 (1 x H), W2^T, b2).
+struct StudentLaunch
+{
+    int            n = 0;
+    int            maxSF = 0;
+    int            maxSlots = 0;
+    int            numElements = 0;
+    int            precision = PREC_FP64;     // type of G and dG/dr
+    int            numSF[kMaxElem] = {};
+    int            numSlots[kMaxElem][kMaxElem] = {};
+    int            hidden[kMaxElem] = {};
+    long           woff1[kMaxElem] = {}, wtoff1[kMaxElem] = {};
+    long           boff1[kMaxElem] = {};
+    long           woff2[kMaxElem] = {}, wtoff2[kMaxElem] = {};
+    long           boff2[kMaxElem] = {};
+    int const*     elem = nullptr;
+    int const*     nbrOff = nullptr;
+    int const*     nbrIdx = nullptr;
+    int const*     nbrCountElem = nullptr;
+    int16_t const* slotSF = nullptr;
+    int const*     atomsByElem = nullptr;
+    ElemStarts     es{};
+    int            blkBeg[kMaxElem + 1] = {}; // gradient blocks per element
+    void const*    G = nullptr;
+    void const*    dGdrSelf = nullptr;
+    void const*    dGdr = nullptr;
+    double const*  Ei = nullptr;              // student atomic energies
+    double const*  F = nullptr;               // student forces [n][3]
+    double const*  labelE = nullptr;          // teacher atomic energies
+    double const*  labelF = nullptr;          // teacher forces [n][3]
+    int const*     batch = nullptr;           // batch atom indices
+    int            batchSize = 0;
+    double         wE = 1.0, wF = 1.0;        // loss weights
+    double         eScale = 1.0;              // Ei units -> label units
+    double         fScale = 1.0;              // chain-rule force -> F units
+    float*         rE = nullptr;              // residuals (0 off the batch)
+    float*         rF = nullptr;
+    float*         u = nullptr;               // adjoint [n][maxSF]
+    float*         blob = nullptr;            // student weights
+    float*         m = nullptr;               // Adam moments (blob layout)
+    float*         v = nullptr;
+    float*         gpart = nullptr;           // [block][paramStride]
+    float*         grad = nullptr;            // summed gradient (blob layout)
+    int            paramStride = 0;
+    double*        loss = nullptr;            // [2] sums of squared residuals
+    float          lr = 1e-3f, beta1 = 0.9f, beta2 = 0.999f, epsAdam = 1e-8f;
+    float          bc1 = 1.0f, bc2 = 1.0f;    // 1 - beta^t (bias correction)
+};
+
+struct RangeLaunch
+{
+    int            maxSF = 0;
+    int            numElements = 0;
+    int            precision = PREC_FP64;
+    int            numSF[kMaxElem] = {};
+    int const*     atomsByElem = nullptr;
+    ElemStarts     es{};
+    int            blkBeg[kMaxElem + 1] = {}; // 256-atom chunks per element
+    void const*    G = nullptr;
+    SFScale const* scale = nullptr;
+    Range*         range = nullptr;           // [element][maxSF], min / max
+};
+
+std::size_t studentGradSmem(int maxNin, int maxH);
+int studentGradBlocks(ElemStarts const& es, int numElements, int* blkBeg);
+void launchStudentTrainStep(StudentLaunch const& L, std::size_t gradSmem,
+                            int maxParams, cudaStream_t s);
+void launchStudentRange(RangeLaunch const& L, cudaStream_t s);
 
 // Forces (chain rule) and energy.
 struct ForceLaunch

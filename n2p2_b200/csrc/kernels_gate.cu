@@ -58,7 +58,7 @@ ewKernel(EWLaunch const L)
             if (L.perAtom) L.perAtom[i] = cnt;
             if (cnt > 0)
             {
-                atomicAdd(&L.status[ST_EW_COUNT], cnt);
+                atomicAdd(&L.status[L.countSlot], cnt);
                 if (L.list)
                 {
                     int const pos = atomicAdd(&L.listCount[e], 1);

@@ -104,18 +104,54 @@ __device__ __forceinline__ void activate(int a, double x, double& v,
     }
 }
 
+__device__ __forceinline__ void activate(int a, float x, float& v, float& dv)
+{
+    float const lim = (float)kExpLimit;
+    switch (a)
+    {
+    case 0: v = x; dv = 1.0f; return;
+    case 1: { float const t = tanhf(x); v = t; dv = 1.0f - t * t; return; }
+    case 2:
+        if (x > lim) { v = 1.0f; dv = 0.0f; return; }
+        if (x < -lim) { v = 0.0f; dv = 0.0f; return; }
+        { float const t = 1.0f / (1.0f + expf(-x)); v = t; dv = t * (1.0f - t); }
+        return;
+    case 3:
+        if (x > lim) { v = x; dv = 1.0f; return; }
+        if (x < -lim) { v = 0.0f; dv = 0.0f; return; }
+        { float const t = expf(x); v = log1pf(t); dv = 1.0f / (1.0f + 1.0f / t); }
+        return;
+    case 4:
+        if (x > 0.0f) { v = x; dv = 1.0f; } else { v = 0.0f; dv = 0.0f; }
+        return;
+    case 5: { float const t = expf(-0.5f * x * x); v = t; dv = -x * t; return; }
+    case 6: v = cosf(x); dv = -sinf(x); return;
+    case 7:
+    { float const t = 1.0f / (1.0f + expf(-x)); v = 1.0f - t; dv = t * (t - 1.0f);
+      return; }
+    case 8: { float const t = expf(-x); v = t; dv = -t; return; }
+    default: v = x * x; dv = 2.0f * x; return;
+    }
+}
+
 // Warp per atom.  Shared memory per warp: activations of the current layer
 // (maxWidth) and the activation derivatives of every layer (L * maxWidth).
+// T = double: the plain form; T = float: the distilled student network.
+template <typename T>
 __global__ void __launch_bounds__(32 * kNNWarps)
-nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
+nnKernel(__grid_constant__ NNParams const P, NNLaunch const L)
 {
-    extern __shared__ double smem[];
+    extern __shared__ double smemD[];
+    T* const smem = reinterpret_cast<T*>(smemD);
+    T const* const weights = static_cast<T const*>(L.weights);
+    T const* const Gin = static_cast<T const*>(L.G);
+    T* const dEdGout = static_cast<T*>(L.dEdG);
     int const lane = threadIdx.x & 31;
     int const w = threadIdx.x >> 5;
     int const W = P.maxWidth;
-    double* x = smem + (long)w * W * (kMaxLayers + 2);
-    double* y = x + W;
-    double* dfs = y + W;  // [layer][W]
+    T* x = smem + (long)w * W * (kMaxLayers + 2);
+    T* y = x + W;
+    T* dfs = y + W;  // [layer][W]
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
     for (int i = blockIdx.x * kNNWarps + w; i < L.n;
          i += gridDim.x * kNNWarps)
@@ -123,24 +159,24 @@ nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
         int const e = L.elem[i];
         int const nl = P.numLayers[e];
         int const nin = P.width[e][0];
-        double const* g = L.G + (long)i * L.maxSF;
+        T const* g = Gin + (long)i * L.maxSF;
         for (int k = lane; k < nin; k += 32) x[k] = g[k];
         __syncwarp();
-        double out = 0.0;
+        T out = T(0);
         for (int l = 1; l < nl; ++l)
         {
             int const ni = P.width[e][l - 1];
             int const no = P.width[e][l];
-            double const* Wt = L.weights + P.wtoff[e][l];
-            double const* b = L.weights + P.boff[e][l];
+            T const* Wt = weights + P.wtoff[e][l];
+            T const* b = weights + P.boff[e][l];
             int const act = P.act[e][l];
             for (int o = lane; o < no; o += 32)
             {
-                double acc = 0.0;
+                T acc = T(0);
                 for (int j = 0; j < ni; ++j) acc += Wt[(long)j * no + o] * x[j];
                 acc += b[o];
                 if (P.normalizeNeurons) acc /= ni;
-                double v, dv;
+                T v, dv;
                 activate(act, acc, v, dv);
                 y[o] = v;
                 dfs[l * W + o] = dv;
@@ -150,16 +186,16 @@ nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
             __syncwarp();
         }
         out = x[0];
-        if (lane == 0) L.energy[i] = out;
+        if (lane == 0) L.energy[i] = (double)out;
         if (L.derivatives)
         {
             // delta_L = f'_L (/ n_{L-1}); delta_{l-1}[j] =
             //   f'_{l-1}[j] * sum_o W_l[o][j] delta_l[o] (/ n_{l-2})
             int const nlast = P.width[e][nl - 2];
-            double* d = y;  // delta of the current layer
+            T* d = y;  // delta of the current layer
             if (lane == 0)
             {
-                double v = dfs[(nl - 1) * W + 0];
+                T v = dfs[(nl - 1) * W + 0];
                 if (P.normalizeNeurons) v /= nlast;
                 d[0] = v;
             }
@@ -168,10 +204,10 @@ nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
             {
                 int const ni = P.width[e][l - 1];
                 int const no = P.width[e][l];
-                double const* Wm = L.weights + P.woff[e][l];
+                T const* Wm = weights + P.woff[e][l];
                 for (int j = lane; j < ni; j += 32)
                 {
-                    double acc = 0.0;
+                    T acc = T(0);
                     for (int o = 0; o < no; ++o)
                         acc += Wm[(long)o * ni + j] * d[o];
                     if (l > 1)
@@ -185,7 +221,7 @@ nnFp64Kernel(__grid_constant__ NNParams const P, NNLaunch const L)
                 for (int j = lane; j < ni; j += 32) d[j] = x[j];
                 __syncwarp();
             }
-            double* o = L.dEdG + (long)i * L.maxSF;
+            T* o = dEdGout + (long)i * L.maxSF;
             for (int k = lane; k < nin; k += 32) o[k] = d[k];
         }
         __syncwarp();
@@ -314,14 +350,27 @@ __global__ void energyKernel(EnergyLaunch const L)
 void launchNeuralNetworks(NNParams const& P, NNLaunch const& L,
                           cudaStream_t s)
 {
-    std::size_t const shm = sizeof(double) * (std::size_t)kNNWarps
-                          * P.maxWidth * (kMaxLayers + 2);
-    cudaFuncSetAttribute(nnFp64Kernel,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (int)shm);
+    bool const f = L.precision != PREC_FP64;
+    std::size_t const shm = (f ? sizeof(float) : sizeof(double))
+                          * (std::size_t)kNNWarps * P.maxWidth
+                          * (kMaxLayers + 2);
     int const grid = (L.n + kNNWarps - 1) / kNNWarps;
     noteLaunches(1);
-    nnFp64Kernel<<<grid > 0 ? grid : 1, 32 * kNNWarps, shm, s>>>(P, L);
+    if (f)
+    {
+        cudaFuncSetAttribute(nnKernel<float>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)shm);
+        nnKernel<float><<<grid > 0 ? grid : 1, 32 * kNNWarps, shm, s>>>(P, L);
+    }
+    else
+    {
+        cudaFuncSetAttribute(nnKernel<double>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)shm);
+        nnKernel<double><<<grid > 0 ? grid : 1, 32 * kNNWarps, shm, s>>>(P,
+                                                                         L);
+    }
 }
 
 void launchForces(ForceLaunch const& L, cudaStream_t s)

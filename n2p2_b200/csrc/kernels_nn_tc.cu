@@ -347,6 +347,18 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
     int const warp = tid >> 5;
     int const lane = tid & 31;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    // Tiles of 128 atoms per element (uniform over the CTA).
+    int tileBeg[kMaxElem + 1];
+    int count[kMaxElem];
+    tileBeg[0] = 0;
+    for (int e = 0; e < P.numElements; ++e)
+    {
+        count[e] = L.listCount ? L.listCount[e]
+                               : L.es.start[e + 1] - L.es.start[e];
+        tileBeg[e + 1] = tileBeg[e] + (count[e] + kTcRows - 1) / kTcRows;
+    }
+    int const total = tileBeg[P.numElements];
+    if ((int)blockIdx.x >= total) return;
 
     uint32_t const bar = smemAddr(sBar);
     if (tid == 0)
@@ -371,14 +383,13 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
     uint32_t const aL = P.split ? smemAddr(sAl) : aH;
     uint32_t phase = 0;
     int loaded = -1;
-    int const total = L.tileBeg[P.numElements];
     bool ok = true;
     int const r = tid;
 
     for (int tile = blockIdx.x; tile < total && ok; tile += gridDim.x)
     {
         int e = 0;
-        while (tile >= L.tileBeg[e + 1]) ++e;
+        while (tile >= tileBeg[e + 1]) ++e;
         TcNet const& N = P.net[e];
         if (e != loaded)
         {
@@ -393,8 +404,8 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
             __syncthreads();
         }
         uint32_t const w0 = smemAddr(sW);
-        int const row0 = L.es.start[e] + (tile - L.tileBeg[e]) * kTcRows;
-        int const rowEnd = L.es.start[e + 1];
+        int const row0 = L.es.start[e] + (tile - tileBeg[e]) * kTcRows;
+        int const rowEnd = L.es.start[e] + count[e];
         bool const valid = row0 + r < rowEnd;
         int const atom = valid ? L.atomsByElem[row0 + r] : -1;
 
@@ -698,7 +709,11 @@ void launchNeuralNetworksTC(TcNNParams const& P, TcNNLaunch const& L,
 {
     cudaFuncSetAttribute(nnTcKernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          P.smemBytes);
-    int const total = L.tileBeg[P.numElements];
+    // Upper bound of the tile count (all atoms); CTAs beyond the actual
+    // count return before allocating tensor memory.
+    int total = 0;
+    for (int e = 0; e < P.numElements; ++e)
+        total += (L.es.start[e + 1] - L.es.start[e] + kTcRows - 1) / kTcRows;
     int const grid = std::max(1, std::min(total, L.grid));
     noteLaunches(1);
     nnTcKernel<<<grid, kTcThreads, P.smemBytes, s>>>(P, L);

@@ -249,6 +249,73 @@ class Mode:
             self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
         return out
 
+    # ---- distilled student ------------------------------------------------
+    _STUDENT_MODES = {"off": _capi.STUDENT_OFF, "gated": _capi.STUDENT_GATED,
+                      "only": _capi.STUDENT_ONLY}
+
+    def setup_student(self, directory: str):
+        """A student potential directory (same symmetry functions and
+        scaling.data, its own weights and training_range.data)."""
+        self._check(self._L.n2p2b_setup_student(self._h, directory.encode()))
+
+    def set_student_mode(self, mode: str):
+        """"off", "gated" (student; teacher for atoms outside the student's
+        training range) or "only"."""
+        self._check(self._L.n2p2b_set_student_mode(
+            self._h, self._STUDENT_MODES[mode]))
+
+    def student_gated_count(self) -> int:
+        c = C.c_int64()
+        self._check(self._L.n2p2b_get_student_gated_count(self._h,
+                                                          C.byref(c)))
+        return int(c.value)
+
+    def student_train_step(self, energy_labels, force_labels, batch,
+                           w_energy=1.0, w_force=1.0, lr=1e-3,
+                           want_loss=False):
+        """One Adam step; labels and batch are CUDA tensors (float64 atomic
+        energies, float64 forces [n, 3], int32 atom indices)."""
+        loss = (C.c_double * 2)() if want_loss else None
+        self._check(self._L.n2p2b_student_train_step(
+            self._h, C.c_void_p(energy_labels.data_ptr()),
+            C.c_void_p(force_labels.data_ptr()), C.c_void_p(batch.data_ptr()),
+            int(batch.numel()), float(w_energy), float(w_force), float(lr),
+            loss))
+        return (loss[0], loss[1]) if want_loss else None
+
+    def student_reset_optimizer(self):
+        self._check(self._L.n2p2b_student_reset_optimizer(self._h))
+
+    def _student_blob(self, which, values=None):
+        size = C.c_int64()
+        self._check(self._L.n2p2b_student_weights(self._h, None, None,
+                                                  C.byref(size), which))
+        if values is None:
+            out = np.zeros(size.value)
+            self._check(self._L.n2p2b_student_weights(
+                self._h, out.ctypes.data_as(C.POINTER(C.c_double)), None,
+                None, which))
+            return out
+        v = np.ascontiguousarray(values, dtype=np.float64)
+        self._check(self._L.n2p2b_student_weights(
+            self._h, None, v.ctypes.data_as(C.POINTER(C.c_double)), None,
+            which))
+
+    def student_weights(self):
+        return self._student_blob(0)
+
+    def set_student_weights(self, blob):
+        self._student_blob(0, blob)
+
+    def student_gradient(self):
+        return self._student_blob(1)
+
+    def student_update_range(self, reset: bool = False):
+        self._check(self._L.n2p2b_student_update_range(self._h, int(reset)))
+
+    def student_write(self, directory: str):
+        self._check(self._L.n2p2b_student_write(self._h, directory.encode()))
+
     _PRECISIONS = {"fp64": _capi.PRECISION_FP64,
                    "mixed": _capi.PRECISION_MIXED,
                    "bf16": _capi.PRECISION_BF16}
