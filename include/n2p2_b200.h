@@ -169,6 +169,40 @@ int n2p2b_evaluate_async(n2p2b_context* ctx, int use_forces);
 /* Waits for the context's stream and reports capacity / invariant flags. */
 int n2p2b_finish(n2p2b_context* ctx);
 
+/* ---- batches of independent structures -------------------------------- */
+
+/* No direct counterpart in the reference, which evaluates one Structure at
+ * a time (nnp-predict's loop over input.data).  Sets num_structures
+ * independent structures in one call: atom_counts[s] atoms each, positions
+ * (sum of counts x 3) and elements concatenated in structure order, boxes
+ * (9 doubles per structure, rows = lattice vectors) or NULL for open
+ * structures.  Every structure gets exactly the neighbor list, energy and
+ * forces it gets alone; one evaluation runs all of them.  Per-atom getters
+ * address the concatenated atoms; n2p2b_get_energy returns the sum. */
+int n2p2b_set_structures(n2p2b_context* ctx, int64_t num_structures,
+                         const int64_t* atom_counts, const double* boxes,
+                         const double* positions, int positions_location,
+                         const int32_t* elements, int flags);
+/* Structure::energy of every structure of the batch (after predict's unit
+ * conversion and offsets); one value for a single structure. */
+int n2p2b_get_structure_energies(n2p2b_context* ctx, double* energies);
+
+/* Captures one whole evaluation (neighbor list to forces, every kernel of
+ * it) into a CUDA graph on the context's stream; n2p2b_launch_graph replays
+ * it with one launch after new positions (n2p2b_set_positions) and
+ * n2p2b_finish checks it.  Changing the structure, precision, student or
+ * statistics settings, or growing a buffer, invalidates the capture. */
+int n2p2b_capture_graph(n2p2b_context* ctx, int use_forces);
+int n2p2b_launch_graph(n2p2b_context* ctx);
+
+/* Autotuner: times every launch configuration (symmetry-function kernel
+ * variant and work ordering, neighbor-list warps per block for batches) on
+ * the current structure(s), keeps the fastest for their size bucket
+ * (log2 atoms per structure, per precision) and applies it to later
+ * structures of that bucket.  `report` receives the choice. */
+int n2p2b_autotune(n2p2b_context* ctx, int use_forces, int repetitions,
+                   char* report, size_t report_len);
+
 /* ---- extrapolation warnings (Element::updateSymmetryFunctionStatistics) */
 
 /* Mode::setupSymmetryFunctionStatistics (libnnp/Mode.cpp:1103-1137): after

@@ -20,6 +20,7 @@
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <map>
 #include <vector>
 
 using namespace n2p2b;
@@ -211,6 +212,19 @@ struct n2p2b_context
     std::vector<SFScale> sfScaleHost;
     DevBuf       ewRange, ewPerAtom;
 
+    // Batch of independent structures (numStructs > 0).
+    long         numStructs = 0;
+    int          batchNIMG = 1;
+    std::vector<BatchStruct> bsHost;
+    std::vector<int64_t> structCounts;
+    DevBuf       structOf, structAtoms, bsDev, structEnergy;
+    int          nlWarpsPerBlock = 4;
+
+    // CUDA graph of one whole evaluation (n2p2b_capture_graph).
+    bool            graphValid = false;
+    bool            graphForces = true;
+    cudaGraphExec_t graphExec = nullptr;
+
     // Distilled student network (FP32, same symmetry functions).
     struct Student
     {
@@ -326,6 +340,9 @@ struct n2p2b_context
             for (auto& e : se.ev) cudaEventDestroy(e);
         for (auto& se : freeEvents)
             for (auto& e : se.ev) cudaEventDestroy(e);
+        if (graphExec) cudaGraphExecDestroy(graphExec);
+        for (DevBuf* b : {&structOf, &structAtoms, &bsDev, &structEnergy})
+            b->release();
         for (DevBuf* b : {&stu.w, &stu.m, &stu.v, &stu.grad, &stu.gpart,
                           &stu.rE,
                           &stu.rF, &stu.u, &stu.loss, &stu.dRange, &stu.list,
@@ -579,6 +596,7 @@ struct n2p2b_context
         for (int k = 0; k < 2; ++k)
         {
             tcGrid[k] = 0;
+            graphValid = false;
             if (!tcOk[k]) continue;
             tcW[k].ensure(tcWeights[k].size());
             ck(cudaMemcpy(tcW[k].p, tcWeights[k].data(), tcWeights[k].size(),
@@ -618,9 +636,164 @@ struct n2p2b_context
 
     // ---- structure -------------------------------------------------------
 
+    // Geometry of one periodic (box != null) or open structure in the
+    // units the kernels compute in.
+    void structureGeometry(double const* box, double rc, NLParams& q,
+                           PhysBox& b, int* cellsOut)
+    {
+        double const L = pot.normalize ? pot.convLength : 1.0;
+        std::memset(&q, 0, sizeof(q));
+        std::memset(&b, 0, sizeof(b));
+        q.rc2 = rc * rc;
+        if (box == nullptr)
+        {
+            q.periodic = 0;
+            q.nimg = 1;
+            if (cellsOut) *cellsOut = 0;
+            return;
+        }
+        for (int k = 0; k < 3; ++k)
+            for (int c = 0; c < 3; ++c) b.box[k][c] = box[3 * k + c];
+        inverseBox(b.box, b.invbox);
+        q.periodic = 1;
+        // Structure::toNormalizedUnits: box *= convLength, invbox /= convL.
+        for (int k = 0; k < 3; ++k)
+            for (int c = 0; c < 3; ++c)
+            {
+                q.box[k][c] = pot.normalize ? b.box[k][c] * L : b.box[k][c];
+                q.invbox[k][c] = pot.normalize ? b.invbox[k][c] / L
+                                               : b.invbox[k][c];
+            }
+        double proj[3];
+        pbcCopies(q.box, rc, q.pbc, proj);
+        q.nimg = (2 * q.pbc[0] + 1) * (2 * q.pbc[1] + 1) * (2 * q.pbc[2] + 1);
+        if (!cellsOut) return;
+        bool cellOk = true;
+        long cells = 1;
+        for (int k = 0; k < 3; ++k)
+        {
+            int nc = (int)std::floor(proj[k] / (rc * (1.0 + 1e-9)));
+            nc = std::min(nc, 160);
+            if (nc < 1 || q.pbc[k] != 1) cellOk = false;
+            q.ncell[k] = nc;
+            cells *= std::max(nc, 1);
+        }
+        if (!cellOk)
+        {
+            q.ncell[0] = q.ncell[1] = q.ncell[2] = 0;
+            *cellsOut = 0;
+        }
+        else *cellsOut = (int)cells;
+    }
+
+    // A batch of independent structures: counts[s] atoms each, boxes
+    // (9 doubles per structure) or null for open structures, positions and
+    // elements concatenated in structure order.
+    void setStructures(long num, int64_t const* counts, double const* boxes,
+                       double const* posArg, int loc, int32_t const* elems,
+                       int flags)
+    {
+        requireReady();
+        if (num <= 0 || !counts || !posArg || !elems)
+            throw std::invalid_argument("ERROR: Invalid batch arguments.\n");
+        long total = 0;
+        for (long s = 0; s < num; ++s)
+        {
+            if (counts[s] <= 0)
+                throw std::invalid_argument("ERROR: Empty structure in "
+                                            "batch.\n");
+            total += counts[s];
+        }
+        if (total > 0x7ffffffeL / 2)
+            throw std::invalid_argument("ERROR: Too many atoms.\n");
+        int const ne = pot.numElements();
+        for (long i = 0; i < total; ++i)
+            if (elems[i] < 0 || elems[i] >= ne)
+                throw std::invalid_argument("ERROR: Element index out of "
+                                            "range.\n");
+        activate();
+        n = total;
+        numStructs = num;
+        sfCap = 0;
+        lastMaxNbr = 0;
+        elemHost.assign(elems, elems + total);
+        periodic = boxes != nullptr;
+        remap = periodic && (flags & N2P2B_REMAP);
+        numCells = 0;
+        std::memset(&nlp, 0, sizeof(nlp));
+        std::memset(&pb, 0, sizeof(pb));
+        double const rc = pot.maxCutoffRadius;
+        bsHost.assign(num, BatchStruct{});
+        structCounts.assign(counts, counts + num);
+        std::vector<int> sOf(total), sAtoms(total);
+        batchNIMG = 1;
+        long a0 = 0;
+        for (long s = 0; s < num; ++s)
+        {
+            BatchStruct& B = bsHost[s];
+            structureGeometry(boxes ? boxes + 9 * s : nullptr, rc, B.p, B.pb,
+                              nullptr);
+            B.doRemap = remap ? 1 : 0;
+            B.atomBeg = (int)a0;
+            B.atomEnd = (int)(a0 + counts[s]);
+            int k = (int)a0;
+            for (int e = 0; e < ne; ++e)
+            {
+                B.es[e] = k;
+                for (long i = a0; i < a0 + counts[s]; ++i)
+                    if (elemHost[i] == e) sAtoms[k++] = (int)i;
+            }
+            for (int e = ne; e <= kMaxElem; ++e) B.es[e] = k;
+            for (long i = a0; i < a0 + counts[s]; ++i) sOf[i] = (int)s;
+            batchNIMG = std::max(batchNIMG, B.p.nimg);
+            a0 += counts[s];
+        }
+        if ((long double)n * batchNIMG * kMaxElem > 1.8e19L)
+            throw std::invalid_argument("ERROR: Batch too large for the "
+                                        "neighbor keys.\n");
+        nlp.nimg = batchNIMG;
+        // Element-sorted atoms of the whole batch (tensor-core tiles,
+        // training blocks).
+        std::vector<int> byElem;
+        byElem.reserve(n);
+        std::memset(&es, 0, sizeof(es));
+        for (int e = 0; e < ne; ++e)
+        {
+            es.start[e] = (int)byElem.size();
+            for (long i = 0; i < n; ++i)
+                if (elemHost[i] == e) byElem.push_back((int)i);
+        }
+        es.start[ne] = (int)byElem.size();
+        for (int e = ne + 1; e <= kMaxElem; ++e) es.start[e] = es.start[ne];
+        posIn.ensure(sizeof(double) * 3 * n);
+        pos.ensure(sizeof(double) * 3 * n);
+        elem.ensure(sizeof(int) * n);
+        atomsByElem.ensure(sizeof(int) * n);
+        structOf.ensure(sizeof(int) * n);
+        structAtoms.ensure(sizeof(int) * n);
+        bsDev.ensure(sizeof(BatchStruct) * num);
+        structEnergy.ensure(sizeof(double) * num);
+        ck(cudaMemcpyAsync(elem.p, elemHost.data(), sizeof(int) * n,
+                           cudaMemcpyHostToDevice, stream), "copy elements");
+        ck(cudaMemcpyAsync(atomsByElem.p, byElem.data(), sizeof(int) * n,
+                           cudaMemcpyHostToDevice, stream), "copy atom lists");
+        ck(cudaMemcpyAsync(structOf.p, sOf.data(), sizeof(int) * n,
+                           cudaMemcpyHostToDevice, stream), "copy batch map");
+        ck(cudaMemcpyAsync(structAtoms.p, sAtoms.data(), sizeof(int) * n,
+                           cudaMemcpyHostToDevice, stream), "copy batch lists");
+        ck(cudaMemcpyAsync(bsDev.p, bsHost.data(), sizeof(BatchStruct) * num,
+                           cudaMemcpyHostToDevice, stream), "copy batch");
+        setPositions(posArg, loc);
+        ck(cudaStreamSynchronize(stream), "batch upload");
+        graphValid = false;
+        applyTuned();
+    }
+
     void setStructure(long num, double const* box, double const* posArg,
                       int loc, int32_t const* elems, int flags)
     {
+        numStructs = 0;
+        graphValid = false;
         requireReady();
         if (num <= 0 || posArg == nullptr || elems == nullptr)
             throw std::invalid_argument("ERROR: Invalid structure "
@@ -718,6 +891,7 @@ struct n2p2b_context
                            cudaMemcpyHostToDevice, stream), "copy atom lists");
         setPositions(posArg, loc);
         ck(cudaStreamSynchronize(stream), "structure upload");
+        applyTuned();
     }
 
     void setPositions(double const* posArg, int loc)
@@ -818,7 +992,9 @@ struct n2p2b_context
         if (mode == precision) return;
         precision = mode;
         sfGrid = 0;
+        graphValid = false;
         invalidate();
+        applyTuned();
         if (n > 0 && !hostOnly())
         {
             activate();
@@ -829,7 +1005,10 @@ struct n2p2b_context
 
     void grow(long total)
     {
-        capacity = std::max(capacity, (long)(total * 1.15) + 1024);
+        // Batches hold tens of millions of entries: keep the headroom small.
+        double const headroom = numStructs > 0 ? 1.02 : 1.15;
+        capacity = std::max(capacity, (long)(total * headroom) + 1024);
+        graphValid = false;
         ensureEntryBuffers();
     }
 
@@ -844,6 +1023,38 @@ struct n2p2b_context
 
     void enqueueNL()
     {
+        if (numStructs > 0)
+        {
+            NLBatchLaunch B;
+            B.n = (int)n;
+            B.numElements = pot.numElements();
+            B.NIMG = batchNIMG;
+            B.capacity = capacity;
+            B.warpsPerBlock = nlWarpsPerBlock;
+            B.normalize = pot.normalize ? 1 : 0;
+            B.convLength = pot.convLength;
+            B.bs = bsDev.as<BatchStruct>();
+            B.structOf = structOf.as<int>();
+            B.structAtoms = structAtoms.as<int>();
+            B.posIn = posIn.as<double>();
+            B.pos = pos.as<double>();
+            B.elem = elem.as<int>();
+            B.nbrCount = nbrCount.as<int>();
+            B.nbrCountElem = nbrCountElem.as<int>();
+            B.nbrOff = nbrOff.as<int>();
+            B.key = key.as<unsigned long long>();
+            B.nbrIdx = nbrIdx.as<int>();
+            B.nbrEl = nbrEl.as<int8_t>();
+            B.dx = dx.as<double>();
+            B.dy = dy.as<double>();
+            B.dz = dz.as<double>();
+            B.dd = dd.as<double>();
+            B.entryAtom = entryAtom.as<int>();
+            B.mirror = mirror.as<int>();
+            B.status = status.as<int>();
+            launchNeighborListBatch(B, stream);
+            return;
+        }
         NLLaunch L;
         L.n = (int)n;
         L.numElements = pot.numElements();
@@ -1153,6 +1364,7 @@ struct n2p2b_context
                                          + ".\n");
         }
         stu.mode = mode;
+        graphValid = false;
         invalidateNN();
     }
 
@@ -1474,6 +1686,23 @@ struct n2p2b_context
 
     void enqueueEnergy()
     {
+        if (numStructs > 0)
+        {
+            BatchEnergyLaunch B;
+            B.numStructs = (int)numStructs;
+            B.numElements = pot.numElements();
+            B.bs = bsDev.as<BatchStruct>();
+            B.atomicEnergy = Ei.as<double>();
+            B.out = structEnergy.as<double>();
+            B.convEnergy = pot.convEnergy;
+            B.meanEnergy = pot.meanEnergy;
+            B.normalize = pot.normalize ? 1 : 0;
+            for (int e = 0; e < pot.numElements(); ++e)
+                B.offset[e] = pot.elements[e].atomicEnergyOffset;
+            B.status = status.as<int>();
+            launchEnergyBatch(B, stream);
+            return;
+        }
         EnergyLaunch L;
         L.n = (int)n;
         L.atomicEnergy = Ei.as<double>();
@@ -1547,6 +1776,7 @@ struct n2p2b_context
         if (sfSharedBytes(sfp, cap, precision) > 227 * 1024)
             throw CapacityError("ERROR: An atom has more neighbors than the "
                                 "symmetry-function kernel can stage.\n");
+        if (cap > sfCap) graphValid = false;
         sfCap = std::max(cap, sfCap);
     }
 
@@ -1663,6 +1893,157 @@ struct n2p2b_context
         return 0;
     }
 
+    // ---- CUDA graph of a whole evaluation ----------------------------------
+
+    void captureGraph(bool forces)
+    {
+        requireReady();
+        requireStructure();
+        if (capacity <= 0 || sfCap <= 0)
+            run(31, forces, forces);       // size every buffer first
+        bool const prof = profiling;
+        profiling = false;
+        // One plain pass fixes the launch configurations (grids, kernel
+        // attributes) and proves the capacities fit.
+        enqueueAll(forces);
+        finishStatus();
+        if (graphExec)
+        {
+            cudaGraphExecDestroy(graphExec);
+            graphExec = nullptr;
+        }
+        graphValid = false;
+        cudaGraph_t g = nullptr;
+        ck(cudaStreamBeginCapture(stream, cudaStreamCaptureModeRelaxed),
+           "begin capture");
+        try
+        {
+            enqueueAll(forces);
+        }
+        catch (...)
+        {
+            cudaStreamEndCapture(stream, &g);
+            if (g) cudaGraphDestroy(g);
+            profiling = prof;
+            throw;
+        }
+        ck(cudaStreamEndCapture(stream, &g), "end capture");
+        cudaError_t const e = cudaGraphInstantiate(&graphExec, g, 0);
+        cudaGraphDestroy(g);
+        profiling = prof;
+        ck(e, "instantiate graph");
+        graphValid = true;
+        graphForces = forces;
+    }
+
+    void launchGraph()
+    {
+        if (!graphValid || !graphExec)
+            throw StateError("ERROR: No valid captured evaluation (capture "
+                             "again after changing the structure, buffers "
+                             "or settings).\n");
+        ck(cudaGraphLaunch(graphExec, stream), "launch graph");
+        invalidate();
+        haveSFDeriv = haveNNDeriv = haveF = graphForces;
+    }
+
+    // ---- autotuner ----------------------------------------------------------
+
+    struct TuneChoice
+    {
+        int variant, sortCats, nlWarps;
+        double ms;
+    };
+    std::map<std::string, TuneChoice> tuned;
+
+    // Size bucket of the current structure(s): log2 of the atoms per
+    // structure, with the precision and the potential's shape.
+    std::string tuneKey() const
+    {
+        long const per = numStructs > 0 ? n / numStructs : n;
+        int b = 0;
+        while ((2L << b) <= per) ++b;
+        return std::to_string(precision) + ":" + std::to_string(maxSF) + ":"
+             + std::to_string(b) + (numStructs > 0 ? ":batch" : "");
+    }
+
+    void applyTuned()
+    {
+        auto it = tuned.find(tuneKey());
+        if (it == tuned.end()) return;
+        sfVariant = it->second.variant;
+        sfSortCats = it->second.sortCats;
+        nlWarpsPerBlock = it->second.nlWarps;
+        sfGrid = 0;
+        graphValid = false;
+    }
+
+    // Times every launch configuration on the current structure(s) and keeps
+    // the fastest for this size bucket.
+    std::string autotune(bool forces, int reps)
+    {
+        requireReady();
+        requireStructure();
+        if (capacity <= 0 || sfCap <= 0) run(31, forces, forces);
+        bool const prof = profiling;
+        profiling = false;
+        std::vector<int> nls = numStructs > 0 ? std::vector<int>{2, 4, 8}
+                                              : std::vector<int>{4};
+        cudaEvent_t a, b;
+        ck(cudaEventCreate(&a), "event");
+        ck(cudaEventCreate(&b), "event");
+        auto timeIt = [&]() {
+            sfGrid = 0;
+            enqueueAll(forces);                 // warm
+            finishStatus();
+            double best = 1e30;
+            for (int r = 0; r < reps; ++r)
+            {
+                ck(cudaEventRecord(a, stream), "record");
+                enqueueAll(forces);
+                ck(cudaEventRecord(b, stream), "record");
+                finishStatus();
+                float ms = 0.0f;
+                ck(cudaEventElapsedTime(&ms, a, b), "elapsed");
+                best = std::min(best, (double)ms);
+            }
+            return best;
+        };
+        if (sfVariant < 0) sfVariant = sfDefaultVariant(sfp);
+        TuneChoice const start{sfVariant, sfSortCats, nlWarpsPerBlock, 0.0};
+        double const t0 = timeIt();
+        TuneChoice best{sfVariant, sfSortCats, nlWarpsPerBlock, t0};
+        std::string rep;
+        for (int v = 0; v < 4; ++v)
+            for (int so = 0; so < 2; ++so)
+                for (int w : nls)
+                {
+                    sfVariant = v;
+                    sfSortCats = so;
+                    nlWarpsPerBlock = w;
+                    double const t = timeIt();
+                    if (t < best.ms) best = TuneChoice{v, so, w, t};
+                }
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+        sfVariant = best.variant;
+        sfSortCats = best.sortCats;
+        nlWarpsPerBlock = best.nlWarps;
+        sfGrid = 0;
+        graphValid = false;
+        profiling = prof;
+        std::string const key = tuneKey();
+        tuned[key] = best;
+        char buf[256];
+        std::snprintf(buf, sizeof(buf),
+                      "bucket %s: sf variant %d, sort %d, nl warps/block %d:"
+                      " %.3f ms per evaluation (start %d/%d/%d: %.3f ms)",
+                      key.c_str(), best.variant, best.sortCats, best.nlWarps,
+                      best.ms, start.variant, start.sortCats, start.nlWarps,
+                      t0);
+        return buf;
+    }
+
     long totalEntries()
     {
         int off = 0;
@@ -1683,7 +2064,8 @@ struct n2p2b_context
         if (E > 0)
             ck(cudaMemcpy(k.data(), key.p, sizeof(unsigned long long) * E,
                           cudaMemcpyDeviceToHost), "read keys");
-        unsigned long long const mod = (unsigned long long)n * nlp.nimg;
+        unsigned long long const mod = (unsigned long long)n
+                                     * (numStructs > 0 ? batchNIMG : nlp.nimg);
         perm.resize(E);
         for (long i = 0; i < n; ++i)
         {
@@ -1952,6 +2334,7 @@ int n2p2b_setup_symmetry_function_statistics(n2p2b_context* ctx,
         if (collect_statistics)
             throw std::invalid_argument("ERROR: Symmetry-function statistics "
                                         "collection is not supported.\n");
+        ctx->graphValid = false;
         ctx->ewCheck = collect_ew || write_ew || stop_on_ew;
         ctx->ewWrite = write_ew != 0;
         ctx->ewStop = stop_on_ew != 0;
@@ -2179,11 +2562,85 @@ int n2p2b_get_energy(n2p2b_context* ctx, double* energy)
         if (!ctx->haveE) throw StateError("ERROR: Energy not calculated.\n");
         if (!energy) throw std::invalid_argument("ERROR: energy");
         ctx->activate();
+        if (ctx->numStructs > 0)
+        {
+            std::vector<double> e(ctx->numStructs);
+            ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+            ck(cudaMemcpy(e.data(), ctx->structEnergy.p,
+                          sizeof(double) * e.size(), cudaMemcpyDeviceToHost),
+               "read energies");
+            double t = 0.0;
+            for (double v : e) t += v;
+            *energy = t;
+            return;
+        }
         ck(cudaMemcpyAsync(ctx->energyHost, ctx->energyOut.p,
                            sizeof(double) * 2, cudaMemcpyDeviceToHost,
                            ctx->stream), "read energy");
         ck(cudaStreamSynchronize(ctx->stream), "synchronize");
         *energy = ctx->energyHost[1];
+    });
+}
+
+int n2p2b_set_structures(n2p2b_context* ctx, int64_t num_structures,
+                         int64_t const* atom_counts, double const* boxes,
+                         double const* positions, int positions_location,
+                         int32_t const* elements, int flags)
+{
+    return guarded(ctx, [&] {
+        ctx->setStructures(num_structures, atom_counts, boxes, positions,
+                           positions_location, elements, flags);
+    });
+}
+
+int n2p2b_get_structure_energies(n2p2b_context* ctx, double* energies)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveE) throw StateError("ERROR: Energy not calculated.\n");
+        if (!energies) throw std::invalid_argument("ERROR: energies");
+        ctx->activate();
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+        if (ctx->numStructs > 0)
+        {
+            ck(cudaMemcpy(energies, ctx->structEnergy.p,
+                          sizeof(double) * ctx->numStructs,
+                          cudaMemcpyDeviceToHost), "read energies");
+            return;
+        }
+        ck(cudaMemcpy(ctx->energyHost, ctx->energyOut.p, sizeof(double) * 2,
+                      cudaMemcpyDeviceToHost), "read energy");
+        energies[0] = ctx->energyHost[1];
+    });
+}
+
+int n2p2b_capture_graph(n2p2b_context* ctx, int use_forces)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        ctx->captureGraph(use_forces != 0);
+    });
+}
+
+int n2p2b_launch_graph(n2p2b_context* ctx)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        ctx->launchGraph();
+    });
+}
+
+int n2p2b_autotune(n2p2b_context* ctx, int use_forces, int repetitions,
+                   char* report, size_t report_len)
+{
+    return guarded(ctx, [&] {
+        ctx->activate();
+        std::string const r = ctx->autotune(use_forces != 0,
+                                            std::max(1, repetitions));
+        if (report && report_len > 0)
+        {
+            std::strncpy(report, r.c_str(), report_len - 1);
+            report[report_len - 1] = '\0';
+        }
     });
 }
 

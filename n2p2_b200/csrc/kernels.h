@@ -60,6 +60,49 @@ void noteLaunches(int k);
 
 void launchNeighborList(NLLaunch const& L, cudaStream_t s);
 
+// One structure of a batch: its geometry and its atoms sorted by element
+// (structAtoms[es[e] .. es[e + 1]) are its atoms of element e, ascending).
+struct BatchStruct
+{
+    NLParams p;
+    PhysBox  pb;
+    int      doRemap;
+    int      atomBeg, atomEnd;       // its atoms in the concatenated arrays
+    int      es[kMaxElem + 1];
+};
+
+struct NLBatchLaunch
+{
+    int                 n = 0;               // atoms of all structures
+    int                 numElements = 0;
+    int                 NIMG = 1;            // largest image count
+    long                capacity = 0;
+    int                 warpsPerBlock = 4;
+    int                 normalize = 0;
+    double              convLength = 1.0;
+    BatchStruct const*  bs = nullptr;
+    int const*          structOf = nullptr;  // [n] structure of each atom
+    int const*          structAtoms = nullptr;
+    double const*       posIn = nullptr;
+    double*             pos = nullptr;
+    int const*          elem = nullptr;
+    int*                nbrCount = nullptr;
+    int*                nbrCountElem = nullptr;
+    int*                nbrOff = nullptr;
+    unsigned long long* key = nullptr;
+    int*                nbrIdx = nullptr;
+    int8_t*             nbrEl = nullptr;
+    double*             dx = nullptr;
+    double*             dy = nullptr;
+    double*             dz = nullptr;
+    double*             dd = nullptr;
+    int*                entryAtom = nullptr;
+    int*                mirror = nullptr;
+    int*                status = nullptr;
+};
+
+void launchNeighborListBatch(NLBatchLaunch const& L, cudaStream_t s);
+
 // Arithmetic of the per-atom stages: the plain form computes everything in
 // FP64.  The mixed forms compute symmetry functions in FP32 and the atomic
 // NNs on the tensor cores with BF16 operands and FP32 accumulation, and keep
@@ -348,5 +391,23 @@ struct EnergyLaunch
 };
 
 void launchEnergy(EnergyLaunch const& L, cudaStream_t s);
+
+// Per-structure energies of a batch: block per structure, fixed-order tree
+// sum, then the conversion and energy offsets of one structure.
+struct BatchEnergyLaunch
+{
+    int                numStructs = 0;
+    int                numElements = 0;
+    BatchStruct const* bs = nullptr;
+    double const*      atomicEnergy = nullptr;
+    double*            out = nullptr;            // [numStructs], physical
+    double             convEnergy = 1.0;
+    double             meanEnergy = 0.0;
+    int                normalize = 0;
+    double             offset[kMaxElem] = {};   // atomic energy offsets
+    int const*         status = nullptr;
+};
+
+void launchEnergyBatch(BatchEnergyLaunch const& L, cudaStream_t s);
 
 } // namespace n2p2b

@@ -565,4 +565,208 @@ void launchNeighborList(NLLaunch const& L, cudaStream_t s)
         L.entryAtom, L.mirror, L.status);
 }
 
+// ===========================================================================
+// Batches of independent structures (one neighbor list per structure, all
+// structures' atoms concatenated).  Every structure keeps its own box and
+// image range; candidates are the atoms of the same structure only, in the
+// brute path's key order, so each structure's list is exactly the one
+// Structure::calculateNeighborList builds for it alone.  Keys use the
+// batch-wide image stride NIMG (the largest structure's image count) so
+// that they stay unique and sorted.
+// ===========================================================================
+
+__global__ void nlbPrepareKernel(int n, double const* __restrict__ posIn,
+                                 int const* __restrict__ structOf,
+                                 BatchStruct const* __restrict__ bs,
+                                 int normalize, double convLength,
+                                 double* __restrict__ pos)
+{
+    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    BatchStruct const& S = bs[structOf[i]];
+    double r[3] = {posIn[3 * i + 0], posIn[3 * i + 1], posIn[3 * i + 2]};
+    if (S.doRemap) remapAtom(r, S.pb.box, S.pb.invbox);
+    if (normalize)
+    {
+        r[0] = __dmul_rn(r[0], convLength);
+        r[1] = __dmul_rn(r[1], convLength);
+        r[2] = __dmul_rn(r[2], convLength);
+    }
+    pos[3 * i + 0] = r[0];
+    pos[3 * i + 1] = r[1];
+    pos[3 * i + 2] = r[2];
+}
+
+// Warp per atom; MODE 0 counts, MODE 1 writes the (sorted) keys.
+template <int MODE>
+__global__ void nlbBruteKernel(int n, int numElements, int NIMG,
+                               double const* __restrict__ pos,
+                               int const* __restrict__ structOf,
+                               BatchStruct const* __restrict__ bs,
+                               int const* __restrict__ structAtoms,
+                               int* __restrict__ nbrCount,
+                               int* __restrict__ nbrCountElem,
+                               int const* __restrict__ nbrOff,
+                               unsigned long long* __restrict__ key,
+                               int const* __restrict__ status)
+{
+    if (status[ST_FLAGS] & FLAG_ABORT) return;
+    int const lane = threadIdx.x & 31;
+    int const i = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    BatchStruct const& S = bs[structOf[i]];
+    NLParams const& p = S.p;
+    double const ri[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    int total = 0;
+    long const base = (MODE == 1) ? (long)nbrOff[i] : 0;
+    int const nimg = p.nimg;
+    for (int e = 0; e < numElements; ++e)
+    {
+        int const eb = S.es[e];
+        long const ncand = (long)(S.es[e + 1] - eb) * nimg;
+        int cntE = 0;
+        for (long c0 = 0; c0 < ncand; c0 += 32)
+        {
+            long const c = c0 + lane;
+            bool hit = false;
+            int j = 0, img = 0;
+            if (c < ncand)
+            {
+                j = structAtoms[eb + (int)(c / nimg)];
+                img = (int)(c % nimg);
+                int b0, b1, b2;
+                imgDecode(p, img, b0, b1, b2);
+                if (!(j == i && b0 == 0 && b1 == 0 && b2 == 0))
+                {
+                    double dr[3];
+                    hit = nlTest(p, ri, pos, j, b0, b1, b2, dr);
+                }
+            }
+            unsigned const m = __ballot_sync(0xffffffffu, hit);
+            if (MODE == 1 && hit)
+            {
+                int const off = total + __popc(m & ((1u << lane) - 1u));
+                key[base + off] = nlKey(e, j, img, n, NIMG);
+            }
+            total += __popc(m);
+            cntE += __popc(m);
+        }
+        if (MODE == 0 && lane == 0)
+            nbrCountElem[(long)i * numElements + e] = cntE;
+    }
+    if (MODE == 0 && lane == 0) nbrCount[i] = total;
+}
+
+__global__ void nlbFinishKernel(int n, int NIMG,
+                                double const* __restrict__ pos,
+                                int const* __restrict__ elem,
+                                int const* __restrict__ structOf,
+                                BatchStruct const* __restrict__ bs,
+                                int const* __restrict__ nbrOff,
+                                unsigned long long const* __restrict__ key,
+                                int* __restrict__ nbrIdx,
+                                int8_t* __restrict__ nbrEl,
+                                double* __restrict__ dx,
+                                double* __restrict__ dy,
+                                double* __restrict__ dz,
+                                double* __restrict__ dd,
+                                int const* __restrict__ status)
+{
+    if (status[ST_FLAGS] & FLAG_ABORT) return;
+    int const lane = threadIdx.x & 31;
+    int const i = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    NLParams const& p = bs[structOf[i]].p;
+    long const b = nbrOff[i];
+    int const cnt = nbrOff[i + 1] - nbrOff[i];
+    double const ri[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    unsigned long long const nimg = (unsigned long long)NIMG;
+    for (int t = lane; t < cnt; t += 32)
+    {
+        unsigned long long const k = key[b + t];
+        int const img = (int)(k % nimg);
+        int const j = (int)((k / nimg) % (unsigned long long)n);
+        int b0, b1, b2;
+        imgDecode(p, img, b0, b1, b2);
+        double dr[3];
+        nlTest(p, ri, pos, j, b0, b1, b2, dr);
+        double const n2 = __dadd_rn(__dadd_rn(__dmul_rn(dr[0], dr[0]),
+                                              __dmul_rn(dr[1], dr[1])),
+                                    __dmul_rn(dr[2], dr[2]));
+        nbrIdx[b + t] = j;
+        nbrEl[b + t] = (int8_t)elem[j];
+        dx[b + t] = dr[0];
+        dy[b + t] = dr[1];
+        dz[b + t] = dr[2];
+        dd[b + t] = __dsqrt_rn(n2);
+    }
+}
+
+__global__ void nlbMirrorKernel(int n, int NIMG,
+                                int const* __restrict__ elem,
+                                int const* __restrict__ structOf,
+                                BatchStruct const* __restrict__ bs,
+                                int const* __restrict__ nbrOff,
+                                unsigned long long const* __restrict__ key,
+                                int const* __restrict__ nbrIdx,
+                                int const* __restrict__ entryAtom,
+                                int* __restrict__ mirror,
+                                int* __restrict__ status)
+{
+    if (status[ST_FLAGS] & FLAG_ABORT) return;
+    long const e = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (e >= (long)nbrOff[n]) return;
+    int const i = entryAtom[e];
+    int const j = nbrIdx[e];
+    int const nimg = bs[structOf[i]].p.nimg;
+    int const img = (int)(key[e] % (unsigned long long)NIMG);
+    unsigned long long const want = nlKey(elem[i], i, nimg - 1 - img, n, NIMG);
+    long lo = nbrOff[j], hi = nbrOff[j + 1];
+    while (lo < hi)
+    {
+        long const mid = (lo + hi) >> 1;
+        if (key[mid] < want) lo = mid + 1;
+        else hi = mid;
+    }
+    if (lo < nbrOff[j + 1] && key[lo] == want)
+    {
+        mirror[e] = (int)lo;
+    }
+    else
+    {
+        mirror[e] = -1;
+        atomicOr(&status[ST_FLAGS], FLAG_MIRROR_MISSING);
+    }
+}
+
+void launchNeighborListBatch(NLBatchLaunch const& L, cudaStream_t s)
+{
+    int const n = L.n;
+    int const tb = 256;
+    int const gAtoms = (n + tb - 1) / tb;
+    int const wpb = L.warpsPerBlock > 0 ? L.warpsPerBlock : 4;
+    int const gWarp = (n + wpb - 1) / wpb;
+    nlbPrepareKernel<<<gAtoms, tb, 0, s>>>(n, L.posIn, L.structOf, L.bs,
+                                           L.normalize, L.convLength, L.pos);
+    nlbBruteKernel<0><<<gWarp, 32 * wpb, 0, s>>>(
+        n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs, L.structAtoms,
+        L.nbrCount, L.nbrCountElem, L.nbrOff, L.key, L.status);
+    nlScanKernel<<<1, 1024, 0, s>>>(n, L.nbrCount, L.nbrOff, L.capacity,
+                                    L.status);
+    nlbBruteKernel<1><<<gWarp, 32 * wpb, 0, s>>>(
+        n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs, L.structAtoms,
+        L.nbrCount, L.nbrCountElem, L.nbrOff, L.key, L.status);
+    nlbFinishKernel<<<gWarp, 32 * wpb, 0, s>>>(
+        n, L.NIMG, L.pos, L.elem, L.structOf, L.bs, L.nbrOff, L.key,
+        L.nbrIdx, L.nbrEl, L.dx, L.dy, L.dz, L.dd, L.status);
+    nlEntryAtomKernel<<<gAtoms, tb, 0, s>>>(n, L.nbrOff, L.entryAtom,
+                                            L.status);
+    long const cap = L.capacity;
+    int const gE = (int)((cap + tb - 1) / tb);
+    noteLaunches(7);
+    nlbMirrorKernel<<<gE > 0 ? gE : 1, tb, 0, s>>>(
+        n, L.NIMG, L.elem, L.structOf, L.bs, L.nbrOff, L.key, L.nbrIdx,
+        L.entryAtom, L.mirror, L.status);
+}
+
 } // namespace n2p2b

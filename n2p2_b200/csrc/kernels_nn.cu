@@ -345,7 +345,45 @@ __global__ void energyKernel(EnergyLaunch const L)
     }
 }
 
+// Block per structure of a batch: the energy kernel's fixed tree over the
+// structure's atoms, then Structure::toPhysicalUnits and
+// Mode::addEnergyOffset for that structure.
+__global__ void energyBatchKernel(BatchEnergyLaunch const L)
+{
+    __shared__ double part[256];
+    int const s = blockIdx.x;
+    if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    BatchStruct const& B = L.bs[s];
+    int const t = threadIdx.x;
+    double v = 0.0;
+    for (int i = B.atomBeg + t; i < B.atomEnd; i += blockDim.x)
+        v += L.atomicEnergy[i];
+    part[t] = v;
+    __syncthreads();
+    for (int h = blockDim.x >> 1; h > 0; h >>= 1)
+    {
+        if (t < h) part[t] += part[t + h];
+        __syncthreads();
+    }
+    if (t == 0)
+    {
+        double e = part[0];
+        if (L.normalize)
+            e = e / L.convEnergy
+              + (double)(B.atomEnd - B.atomBeg) * L.meanEnergy;
+        for (int k = 0; k < L.numElements; ++k)
+            e += (double)(B.es[k + 1] - B.es[k]) * L.offset[k];
+        L.out[s] = e;
+    }
+}
+
 } // namespace
+
+void launchEnergyBatch(BatchEnergyLaunch const& L, cudaStream_t s)
+{
+    noteLaunches(1);
+    energyBatchKernel<<<L.numStructs > 0 ? L.numStructs : 1, 256, 0, s>>>(L);
+}
 
 void launchNeuralNetworks(NNParams const& P, NNLaunch const& L,
                           cudaStream_t s)

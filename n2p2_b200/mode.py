@@ -178,6 +178,50 @@ class Mode:
         self.num_atoms = n
         del keep
 
+    def set_structures(self, structures, remap: bool = True):
+        """A batch of independent structures, each (box or None, positions,
+        elements); evaluated together, each exactly as alone."""
+        counts = np.array([len(s[1]) for s in structures], dtype=np.int64)
+        pos = np.ascontiguousarray(np.concatenate([s[1] for s in structures]),
+                                   dtype=np.float64)
+        el = np.ascontiguousarray(np.concatenate([s[2] for s in structures]),
+                                  dtype=np.int32)
+        periodic = [s[0] is not None for s in structures]
+        if any(periodic) and not all(periodic):
+            raise ValueError("a batch is all periodic or all open")
+        bp = None
+        if all(periodic):
+            boxes = np.ascontiguousarray(
+                np.stack([np.asarray(s[0], dtype=np.float64).reshape(9)
+                          for s in structures]))
+            bp = boxes.ctypes.data_as(C.c_void_p)
+        self._check(self._L.n2p2b_set_structures(
+            self._h, len(structures),
+            counts.ctypes.data_as(C.POINTER(C.c_int64)), bp,
+            pos.ctypes.data_as(C.c_void_p), _capi.HOST,
+            el.ctypes.data_as(C.POINTER(C.c_int32)),
+            _capi.REMAP if remap else 0))
+        self.num_atoms = int(counts.sum())
+        self.num_structures = len(structures)
+
+    def structure_energies(self):
+        out = np.zeros(getattr(self, "num_structures", 1))
+        self._check(self._L.n2p2b_get_structure_energies(
+            self._h, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return out
+
+    def capture_graph(self, use_forces: bool = True):
+        self._check(self._L.n2p2b_capture_graph(self._h, int(use_forces)))
+
+    def launch_graph(self):
+        self._check(self._L.n2p2b_launch_graph(self._h))
+
+    def autotune(self, use_forces: bool = True, repetitions: int = 3) -> str:
+        buf = C.create_string_buffer(512)
+        self._check(self._L.n2p2b_autotune(self._h, int(use_forces),
+                                           int(repetitions), buf, 512))
+        return buf.value.decode()
+
     def set_positions(self, positions):
         p, loc, keep = _ptr_and_loc(positions, np.float64)
         self._check(self._L.n2p2b_set_positions(self._h, p, loc))

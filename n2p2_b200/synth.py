@@ -110,11 +110,62 @@ def noisy_frames(pos: np.ndarray, n_frames: int, sigma: float, seed: int,
 
 
 def batch_structures(n_structures: int, seed: int, lo: int = 11,
-                     hi: int = 171):
-    """Independent water boxes with N ~ U[lo, hi] molecules each."""
+                     hi: int = 171, device: str = "cpu"):
+    """Independent water boxes with N ~ U[lo, hi] molecules each (density
+    1.0 g/cm^3, O-O >= 4.7 bohr, seeded orientations), built by random
+    sequential addition run for all structures at once with torch on
+    `device`: every round proposes one oxygen per unfinished structure and
+    accepts it if it keeps the minimum distance (minimum image) to the
+    oxygens placed so far.  Returns a list of (box, positions, elements)."""
+    import torch
     rng = np.random.default_rng(seed)
     counts = rng.integers(lo, hi + 1, size=n_structures)
+    dev = torch.device(device)
+    g = torch.Generator(device=dev)
+    g.manual_seed(int(seed))
+    S = n_structures
+    nmax = int(counts.max())
+    L = torch.tensor([box_length(int(c)) for c in counts],
+                     dtype=torch.float64, device=dev)
+    cnt = torch.tensor(counts, dtype=torch.int64, device=dev)
+    placed = torch.zeros((S, nmax, 3), dtype=torch.float64, device=dev)
+    npl = torch.zeros(S, dtype=torch.int64, device=dev)
+    slot = torch.arange(nmax, device=dev)
+    min2 = MIN_OO_BOHR ** 2
+    rounds = 0
+    while True:
+        act = torch.nonzero(npl < cnt).flatten()
+        if act.numel() == 0:
+            break
+        rounds += 1
+        if rounds > 200000:
+            raise RuntimeError("water placement did not converge")
+        La = L[act]
+        cand = torch.rand((act.numel(), 3), generator=g, dtype=torch.float64,
+                          device=dev) * La[:, None]
+        d = cand[:, None, :] - placed[act]
+        d -= La[:, None, None] * torch.round(d / La[:, None, None])
+        bad = ((d * d).sum(-1) < min2) & (slot[None, :] < npl[act, None])
+        ok = ~bad.any(dim=1)
+        acc = act[ok]
+        placed[acc, npl[acc]] = cand[ok]
+        npl[acc] += 1
+    u = torch.randn((S, nmax, 3), generator=g, dtype=torch.float64,
+                    device=dev)
+    u /= torch.linalg.norm(u, dim=2, keepdim=True)
+    v = torch.randn((S, nmax, 3), generator=g, dtype=torch.float64,
+                    device=dev)
+    v -= (v * u).sum(dim=2, keepdim=True) * u
+    v /= torch.linalg.norm(v, dim=2, keepdim=True)
+    th = math.radians(HOH_DEG)
+    h1 = placed + OH_BOHR * u
+    h2 = placed + OH_BOHR * (math.cos(th) * u + math.sin(th) * v)
+    allpos = torch.stack([placed, h1, h2], dim=2).cpu().numpy()
+    Ls = L.cpu().numpy()
     out = []
-    for k, n in enumerate(counts):
-        out.append(water_box(int(n), seed * 100003 + k))
+    for k in range(S):
+        n = int(counts[k])
+        pos = allpos[k, :n].reshape(-1, 3)
+        elem = np.tile(np.array([O, H, H], dtype=np.int32), n)
+        out.append((np.eye(3) * Ls[k], pos, elem))
     return out
