@@ -75,6 +75,8 @@ def args():
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-forms", action="store_true",
                    help="skip the mixed-precision comparison")
+    a.add_argument("--no-batch", action="store_true",
+                   help="skip the 4,096-structure batching form")
     return a.parse_args()
 
 
@@ -430,6 +432,74 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
     return out
 
 
+def measure_batch(stream, lib, local, n_structures=4096, steps=5):
+    """Batching form: 4,096 independent water boxes of 11-171 molecules
+    (33-513 atoms, density 1.0 g/cm^3), evaluated together as one CUDA-graph
+    launch after the autotuner picked the launch configuration for their
+    size bucket (tuned on a 256-structure sample of the same distribution).
+    Compared with a loop that evaluates one structure per call."""
+    import torch
+    from n2p2_b200 import synth
+    from n2p2_b200.mode import Prediction
+    t0 = time.perf_counter()
+    structs = synth.batch_structures(n_structures, 2027, device=f"cuda:{local}")
+    sample = synth.batch_structures(256, 2028, device=f"cuda:{local}")
+    gen_s = time.perf_counter() - t0
+    natoms = sum(len(s[2]) for s in structs)
+    out = {"structures": n_structures, "atoms": natoms,
+           "atoms_per_structure": [int(min(len(s[2]) for s in structs)),
+                                   int(max(len(s[2]) for s in structs))],
+           "generation_s": gen_s}
+    p = Prediction(POT, device=local)
+    p.setup()
+    p.setup_symmetry_function_statistics(False, False, False, False)
+    p.set_stream(stream.cuda_stream)
+    for prec in ("fp64", "mixed"):
+        p.set_precision(prec)
+        p.set_structures(sample)
+        p.evaluate_nnp(True)
+        tune = p.autotune(True, 1)
+        p.set_structures(structs)
+        p.evaluate_nnp(True)
+        p.capture_graph(True)
+        p.launch_graph()
+        p.finish()
+        ev0 = torch.cuda.Event(enable_timing=True)
+        ev1 = torch.cuda.Event(enable_timing=True)
+        l0 = lib.n2p2b_kernel_launch_count()
+        ev0.record(stream)
+        for _ in range(steps):
+            p.launch_graph()
+        ev1.record(stream)
+        p.finish()
+        t = ev0.elapsed_time(ev1) / 1e3
+        out[prec] = {"value": natoms * steps / t, "unit": "atoms/s",
+                     "ms_per_batch": 1e3 * t / steps, "steps": steps,
+                     "graph_launches_per_batch": 1,
+                     "kernels_per_batch": (lib.n2p2b_kernel_launch_count()
+                                           - l0) / steps,
+                     "autotune": tune}
+    # One structure per call (set_structure + evaluate), on a sample.
+    p.set_precision("fp64")
+    k = 512
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    na = 0
+    for box, x, el in structs[:k]:
+        p.set_structure(x, el, box)
+        p.evaluate_nnp(True)
+        na += len(el)
+    p.finish()
+    t = time.perf_counter() - t0
+    out["loop_fp64"] = {"value": na / t, "unit": "atoms/s",
+                        "sample": f"first {k} structures, one "
+                                  "set_structure + evaluate per structure"}
+    out["speedup_fp64_vs_loop"] = out["fp64"]["value"] / out["loop_fp64"][
+        "value"]
+    p.close()
+    return out
+
+
 def run_ours(a):
     import torch
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -510,6 +580,9 @@ def run_ours(a):
         if world == 1 and not a.no_forms:
             forms = measure_forms(box, frames, elem, dev_frames, stream, lib,
                                   min(a.steps, 50), local)
+        batch = None
+        if world == 1 and not a.no_batch:
+            batch = measure_batch(stream, lib, local)
 
     if dist is not None:
         dist.barrier()
@@ -565,6 +638,8 @@ def run_ours(a):
     }
     if forms is not None:
         line["forms"] = forms
+    if batch is not None:
+        line["batch"] = batch
     if not a.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(frames, box, elem)
     print(json.dumps(line))
