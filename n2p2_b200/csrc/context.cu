@@ -1822,6 +1822,9 @@ struct n2p2b_context
             if (flags & FLAG_TC_TIMEOUT)
                 throw CudaError("ERROR: A tensor-core wait of the NN kernel "
                                 "gave up; results are invalid.\n");
+            if (flags & FLAG_SF_PATH)
+                throw std::runtime_error("ERROR: Internal: symmetry-function "
+                                         "kernel without a needed path.\n");
             if (sizing || (flags & FLAG_SF_CAPACITY))
             {
                 fitSFCap(statusHost[ST_MAX_NBR]);
@@ -1888,6 +1891,9 @@ struct n2p2b_context
         if (flags & FLAG_TC_TIMEOUT)
             throw CudaError("ERROR: A tensor-core wait of the NN kernel gave "
                             "up; results are invalid.\n");
+        if (flags & FLAG_SF_PATH)
+            throw std::runtime_error("ERROR: Internal: symmetry-function "
+                                     "kernel without a needed path.\n");
         haveNL = haveSF = haveNN = haveE = true;
         if (ewCheck) accountEW();
         return 0;

@@ -29,7 +29,8 @@ enum StatusFlags
                                   // kernel's shared-memory staging holds
     FLAG_MIRROR_MISSING = 1 << 3, // mirror entry not found (invariant broken)
     FLAG_ABORT         = 1 << 4,  // stop: later kernels return immediately
-    FLAG_TC_TIMEOUT    = 1 << 5   // a tensor-core wait gave up (bounded)
+    FLAG_TC_TIMEOUT    = 1 << 5,  // a tensor-core wait gave up (bounded)
+    FLAG_SF_PATH       = 1 << 6   // SF kernel lacks a needed code path
 };
 
 // Physical-unit box used by Structure::remap (before normalization).

@@ -11,7 +11,7 @@ namespace n2p2b
 #define N2P2B_SF_DECL(SUFFIX)                                                 \
     void sfLaunch_##SUFFIX(SFParams const&, SFLaunch const&, std::size_t,     \
                            cudaStream_t, int);                                \
-    int sfBlocks_##SUFFIX(std::size_t, int);
+    int sfBlocks_##SUFFIX(SFParams const&, std::size_t, int);
 N2P2B_SF_DECL(1)
 N2P2B_SF_DECL(2)
 N2P2B_SF_DECL(6)
@@ -51,11 +51,11 @@ int sfBlocksPerSM(SFParams const& P, int cap, int variant, int precision)
     bool const f = precision != PREC_FP64;
     switch (P.cutoffType)
     {
-    case 1: return f ? sfBlocks_1f(shm, variant) : sfBlocks_1(shm, variant);
-    case 2: return f ? sfBlocks_2f(shm, variant) : sfBlocks_2(shm, variant);
-    case 6: return f ? sfBlocks_6f(shm, variant) : sfBlocks_6(shm, variant);
+    case 1: return f ? sfBlocks_1f(P, shm, variant) : sfBlocks_1(P, shm, variant);
+    case 2: return f ? sfBlocks_2f(P, shm, variant) : sfBlocks_2(P, shm, variant);
+    case 6: return f ? sfBlocks_6f(P, shm, variant) : sfBlocks_6(P, shm, variant);
     default:
-        return f ? sfBlocks_anyf(shm, variant) : sfBlocks_any(shm, variant);
+        return f ? sfBlocks_anyf(P, shm, variant) : sfBlocks_any(P, shm, variant);
     }
 }
 

@@ -12,9 +12,9 @@ void sfLaunch_any(SFParams const& P, SFLaunch const& L, std::size_t shm,
     sfk::launchForCT<double, -1>(P, L, shm, s, variant);
 }
 
-int sfBlocks_any(std::size_t shm, int variant)
+int sfBlocks_any(SFParams const& P, std::size_t shm, int variant)
 {
-    return sfk::blocksForCT<double, -1>(shm, variant);
+    return sfk::blocksForCT<double, -1>(P, shm, variant);
 }
 
 } // namespace n2p2b

@@ -12,9 +12,9 @@ void sfLaunch_1f(SFParams const& P, SFLaunch const& L, std::size_t shm,
     sfk::launchForCT<float, 1>(P, L, shm, s, variant);
 }
 
-int sfBlocks_1f(std::size_t shm, int variant)
+int sfBlocks_1f(SFParams const& P, std::size_t shm, int variant)
 {
-    return sfk::blocksForCT<float, 1>(shm, variant);
+    return sfk::blocksForCT<float, 1>(P, shm, variant);
 }
 
 } // namespace n2p2b

@@ -12,9 +12,9 @@ void sfLaunch_6(SFParams const& P, SFLaunch const& L, std::size_t shm,
     sfk::launchForCT<double, 6>(P, L, shm, s, variant);
 }
 
-int sfBlocks_6(std::size_t shm, int variant)
+int sfBlocks_6(SFParams const& P, std::size_t shm, int variant)
 {
-    return sfk::blocksForCT<double, 6>(shm, variant);
+    return sfk::blocksForCT<double, 6>(P, shm, variant);
 }
 
 } // namespace n2p2b

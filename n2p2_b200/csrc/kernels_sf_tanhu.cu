@@ -12,9 +12,9 @@ void sfLaunch_2(SFParams const& P, SFLaunch const& L, std::size_t shm,
     sfk::launchForCT<double, 2>(P, L, shm, s, variant);
 }
 
-int sfBlocks_2(std::size_t shm, int variant)
+int sfBlocks_2(SFParams const& P, std::size_t shm, int variant)
 {
-    return sfk::blocksForCT<double, 2>(shm, variant);
+    return sfk::blocksForCT<double, 2>(P, shm, variant);
 }
 
 } // namespace n2p2b

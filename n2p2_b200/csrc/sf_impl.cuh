@@ -51,6 +51,8 @@
 // the force kernel loads, coalesced.
 #pragma once
 
+#include <cstdlib>
+
 #include "device_common.cuh"
 #include "kernels.h"
 
@@ -805,7 +807,22 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
     }
 }
 
-template <typename R, int CT, int NS, int NRC>
+// N2P2B_SF_PATHS=31 forces the kernel with every path (A/B measurements).
+inline int L_pathsOverride()
+{
+    static int const v = [] {
+        char const* e = std::getenv("N2P2B_SF_PATHS");
+        return e ? std::atoi(e) : 0;
+    }();
+    return v;
+}
+
+// Code paths compiled into a kernel instantiation (a kernel holding only the
+// paths a potential uses is smaller and misses the instruction cache less).
+constexpr int kPathRadial = 1, kPathFastNarrow = 2, kPathFastWide = 4,
+              kPathGenNarrow = 8, kPathGenWide = 16, kPathAll = 31;
+
+template <typename R, int CT, int NS, int NRC, int PATHS>
 __global__ void __launch_bounds__(kThreads)
 sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 {
@@ -973,24 +990,49 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             }
             __syncwarp();
             if (h.type == 2)
-                radialSegment<R, kGenericChunk>(sG, sM, g0, g1, eb, cnt, W,
-                                                out, L.derivatives);
+            {
+                if (PATHS & kPathRadial)
+                    radialSegment<R, kGenericChunk>(sG, sM, g0, g1, eb, cnt,
+                                                    W, out, L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
             else if (fast && h.type == 3)
-                angularFast<R, CT, NS, NRC, true>(P, sG, sM, g0, g1, eb, cnt,
-                                                  words, cap, W, out,
-                                                  L.derivatives);
+            {
+                if (PATHS & kPathFastNarrow)
+                    angularFast<R, CT, NS, NRC, true>(P, sG, sM, g0, g1, eb,
+                                                      cnt, words, cap, W, out,
+                                                      L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
             else if (fast)
-                angularFast<R, CT, NS, NRC, false>(P, sG, sM, g0, g1, eb, cnt,
-                                                   words, cap, W, out,
-                                                   L.derivatives);
+            {
+                if (PATHS & kPathFastWide)
+                    angularFast<R, CT, NS, NRC, false>(P, sG, sM, g0, g1, eb,
+                                                       cnt, words, cap, W,
+                                                       out, L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
             else if (h.type == 3)
-                angularGeneric<R, CT, kGenericChunk, true>(
-                    P, sG, sM, g0, g1, eb, cnt, words, cap, W, out,
-                    L.derivatives);
+            {
+                if (PATHS & kPathGenNarrow)
+                    angularGeneric<R, CT, kGenericChunk, true>(
+                        P, sG, sM, g0, g1, eb, cnt, words, cap, W, out,
+                        L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
             else
-                angularGeneric<R, CT, kGenericChunk, false>(
-                    P, sG, sM, g0, g1, eb, cnt, words, cap, W, out,
-                    L.derivatives);
+            {
+                if (PATHS & kPathGenWide)
+                    angularGeneric<R, CT, kGenericChunk, false>(
+                        P, sG, sM, g0, g1, eb, cnt, words, cap, W, out,
+                        L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
             __syncwarp();
             g0 = g1;
         }
@@ -1014,24 +1056,76 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     }
 }
 
+// Paths a potential needs for shape count NS: the kernel's own segment
+// rule (consecutive groups of equal (type, rc), at most kMaxSegGroups; fast
+// only if every group of the segment has NS shapes).
+inline int pathsNeeded(SFParams const& P, int NS)
+{
+    int paths = 0;
+    for (int e = 0; e < P.numElements; ++e)
+    {
+        int g0 = P.groupBeg[e];
+        int const ge = P.groupBeg[e + 1];
+        while (g0 < ge)
+        {
+            DevGroup const& h = P.groups[g0];
+            int g1 = g0 + 1;
+            bool fast = (h.type != 2) && (h.shapes == NS);
+            while (g1 < ge && P.groups[g1].type == h.type
+                   && P.groups[g1].rc == h.rc && g1 - g0 < kMaxSegGroups)
+            {
+                fast = fast && (P.groups[g1].shapes == NS);
+                ++g1;
+            }
+            if (h.type == 2) paths |= kPathRadial;
+            else if (fast) paths |= (h.type == 3) ? kPathFastNarrow
+                                                  : kPathFastWide;
+            else paths |= (h.type == 3) ? kPathGenNarrow : kPathGenWide;
+            g0 = g1;
+        }
+    }
+    return paths;
+}
+
 // Launch and occupancy helpers for one cutoff type; variant = (NS, NRC).
+// Potentials of radial + product-form narrow angular groups (the usual
+// layout) get the kernel without the other paths.
+constexpr int kPathsCommon = kPathRadial | kPathFastNarrow;
+
+inline bool useCommonPaths(SFParams const& P, int NS)
+{
+    int const need = pathsNeeded(P, NS);
+    return (need & ~kPathsCommon) == 0 && L_pathsOverride() != kPathAll;
+}
+
 template <typename R, int CT, int NS, int NRC>
 void launchVariant(SFParams const& P, SFLaunch const& L, std::size_t shm,
                    cudaStream_t s)
 {
-    cudaFuncSetAttribute(sfKernel<R, CT, NS, NRC>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
-    sfKernel<R, CT, NS, NRC><<<L.grid, kThreads, shm, s>>>(P, L);
+    if (useCommonPaths(P, NS))
+    {
+        auto k = sfKernel<R, CT, NS, NRC, kPathsCommon>;
+        cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)shm);
+        k<<<L.grid, kThreads, shm, s>>>(P, L);
+        return;
+    }
+    auto k = sfKernel<R, CT, NS, NRC, kPathAll>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)shm);
+    k<<<L.grid, kThreads, shm, s>>>(P, L);
 }
 
 template <typename R, int CT, int NS, int NRC>
-int blocksVariant(std::size_t shm)
+int blocksVariant(SFParams const& P, std::size_t shm)
 {
-    cudaFuncSetAttribute(sfKernel<R, CT, NS, NRC>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)shm);
+    auto k = useCommonPaths(P, NS) ? sfKernel<R, CT, NS, NRC, kPathsCommon>
+                                   : sfKernel<R, CT, NS, NRC, kPathAll>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)shm);
     int blocks = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-            &blocks, sfKernel<R, CT, NS, NRC>, kThreads, shm) != cudaSuccess
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k, kThreads,
+                                                      shm) != cudaSuccess
         || blocks < 1)
         blocks = 1;
     return blocks;
@@ -1052,14 +1146,14 @@ void launchForCT(SFParams const& P, SFLaunch const& L, std::size_t shm,
 }
 
 template <typename R, int CT>
-int blocksForCT(std::size_t shm, int variant)
+int blocksForCT(SFParams const& P, std::size_t shm, int variant)
 {
     switch (variant)
     {
-    case 1: return blocksVariant<R, CT, 4, 1>(shm);
-    case 2: return blocksVariant<R, CT, 8, 1>(shm);
-    case 3: return blocksVariant<R, CT, 8, 2>(shm);
-    default: return blocksVariant<R, CT, 4, 3>(shm);
+    case 1: return blocksVariant<R, CT, 4, 1>(P, shm);
+    case 2: return blocksVariant<R, CT, 8, 1>(P, shm);
+    case 3: return blocksVariant<R, CT, 8, 2>(P, shm);
+    default: return blocksVariant<R, CT, 4, 3>(P, shm);
     }
 }
 
