@@ -114,6 +114,13 @@ int    n2p2b_num_symmetry_functions(const n2p2b_context* ctx, int e);
 int    n2p2b_num_slots(const n2p2b_context* ctx, int e, int ne);
 /* Mode::getMaxCutoffRadius (normalized units, libnnp/Mode.h:693). */
 double n2p2b_max_cutoff_radius(const n2p2b_context* ctx);
+/* Element::getAtomicEnergyOffset and atomic number of element e. */
+double n2p2b_atomic_energy_offset(const n2p2b_context* ctx, int e);
+int    n2p2b_atomic_number(const n2p2b_context* ctx, int e);
+/* mean_energy, conv_energy, conv_length of input.nn (1 / 0 when the
+ * potential does not normalize); returns 1 if it normalizes. */
+int    n2p2b_unit_conversion(const n2p2b_context* ctx, double* mean_energy,
+                             double* conv_energy, double* conv_length);
 /* Parameters of symmetry function s (sorted index = NN input index) of
  * element e, as Element::getSymmetryFunction(s) holds them (normalized
  * units): out[0..9] = type, e1, e2 (-1 for radial), eta, rs, rc, zeta,
@@ -168,6 +175,32 @@ int n2p2b_evaluate(n2p2b_context* ctx, int use_forces);
 int n2p2b_evaluate_async(n2p2b_context* ctx, int use_forces);
 /* Waits for the context's stream and reports capacity / invariant flags. */
 int n2p2b_finish(n2p2b_context* ctx);
+
+/* ---- neighbor list supplied by an MD engine (InterfaceLammps) ---------- */
+
+/* InterfaceLammps::setLocalAtoms + allocateNeighborlists + addNeighbor +
+ * finalizeNeighborList (libnnpif/LAMMPS/InterfaceLammps.cpp:267-304,
+ * 400-457) in one call: num_atoms local atoms with their element indices;
+ * atom i has neighbor_counts[i] entries (concatenated over atoms) with the
+ * neighbor's position in the engine's force array (local atoms first, then
+ * ghost atoms; num_targets in all), its element index and
+ * dr = r_i - r_neighbor in the potential's physical units (the engine
+ * converts by cflength first).  The library builds no neighbor list of its
+ * own; the next evaluation (InterfaceLammps::process, libnnpif/LAMMPS/
+ * InterfaceLammps.cpp:463-487) uses this one, and n2p2b_get_energy returns
+ * the local atoms' energy. */
+int n2p2b_set_neighbor_list(n2p2b_context* ctx, int64_t num_atoms,
+                            const int32_t* elements,
+                            const int64_t* neighbor_counts,
+                            const int64_t* neighbor_index,
+                            const int32_t* neighbor_elements,
+                            const double* dr, int64_t num_targets);
+/* InterfaceLammps::getForces (libnnpif/LAMMPS/InterfaceLammps.cpp:533-581):
+ * forces on all num_targets local and ghost atoms (num_targets x 3,
+ * overwritten; the engine adds them to its own force array), physical
+ * units: each local atom's self term plus every pair term pointing at the
+ * target, summed in a fixed order. */
+int n2p2b_get_target_forces(n2p2b_context* ctx, double* forces);
 
 /* ---- batches of independent structures -------------------------------- */
 

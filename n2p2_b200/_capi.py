@@ -76,6 +76,12 @@ SIGNATURES = {
     "n2p2b_num_symmetry_functions": (C.c_int, [_vp, C.c_int]),
     "n2p2b_num_slots": (C.c_int, [_vp, C.c_int, C.c_int]),
     "n2p2b_max_cutoff_radius": (C.c_double, [_vp]),
+    "n2p2b_atomic_energy_offset": (C.c_double, [_vp, C.c_int]),
+    "n2p2b_atomic_number": (C.c_int, [_vp, C.c_int]),
+    "n2p2b_unit_conversion": (C.c_int, [_vp, _dp, _dp, _dp]),
+    "n2p2b_set_neighbor_list": (C.c_int, [_vp, C.c_int64, _i32p, _i64p,
+                                          _i64p, _i32p, _dp, C.c_int64]),
+    "n2p2b_get_target_forces": (C.c_int, [_vp, _dp]),
     "n2p2b_symmetry_function_params": (C.c_int, [_vp, C.c_int, C.c_int, _dp]),
     "n2p2b_num_groups": (C.c_int, [_vp, C.c_int]),
     "n2p2b_group_members": (C.c_int, [_vp, C.c_int, C.c_int, _i32p, C.c_int]),

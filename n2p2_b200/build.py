@@ -84,9 +84,38 @@ def build(verbose: bool = False, ptxas_info: bool = False) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed:\n{r.stderr}")
+    build_apps()
     if verbose:
         print(LIB)
     return LIB
+
+
+APPS = {"nnp-predict": "nnp_predict.cpp", "lammps-emulate": "lammps_emulate.cpp"}
+
+
+def build_apps() -> list[str]:
+    """The command-line programs (n2p2_b200/bin/): host C++ over the C-ABI,
+    linked against the in-tree library (rpath $ORIGIN/..)."""
+    out_dir = os.path.join(PKG, "bin")
+    os.makedirs(out_dir, exist_ok=True)
+    out = []
+    for name, src in APPS.items():
+        srcp = os.path.join(PKG, "apps", src)
+        exe = os.path.join(out_dir, name)
+        deps = [srcp, LIB, os.path.join(ROOT, "include", "n2p2_b200.h"),
+                os.path.join(ROOT, "include", "n2p2_b200.hpp")]
+        if (not os.path.exists(exe)
+                or any(os.path.getmtime(d) > os.path.getmtime(exe)
+                       for d in deps)):
+            cmd = ["g++", "-std=c++17", "-O2", "-I" + os.path.join(ROOT,
+                                                                  "include"),
+                   srcp, "-L" + PKG, "-ln2p2b200",
+                   "-Wl,-rpath,$ORIGIN/..", "-o", exe]
+            r = subprocess.run(cmd, capture_output=True, text=True)
+            if r.returncode != 0:
+                raise RuntimeError(f"g++ failed for {src}:\n{r.stderr}")
+        out.append(exe)
+    return out
 
 
 if __name__ == "__main__":

@@ -212,6 +212,11 @@ struct n2p2b_context
     std::vector<SFScale> sfScaleHost;
     DevBuf       ewRange, ewPerAtom;
 
+    // Externally supplied neighbor list (n2p2b_set_neighbor_list).
+    bool         externalNL = false;
+    long         numTargets = 0;
+    DevBuf       revOff, revEntry, Ftarget;
+
     // Batch of independent structures (numStructs > 0).
     long         numStructs = 0;
     int          batchNIMG = 1;
@@ -341,7 +346,8 @@ struct n2p2b_context
         for (auto& se : freeEvents)
             for (auto& e : se.ev) cudaEventDestroy(e);
         if (graphExec) cudaGraphExecDestroy(graphExec);
-        for (DevBuf* b : {&structOf, &structAtoms, &bsDev, &structEnergy})
+        for (DevBuf* b : {&structOf, &structAtoms, &bsDev, &structEnergy,
+                          &revOff, &revEntry, &Ftarget})
             b->release();
         for (DevBuf* b : {&stu.w, &stu.m, &stu.v, &stu.grad, &stu.gpart,
                           &stu.rE,
@@ -714,6 +720,7 @@ struct n2p2b_context
         activate();
         n = total;
         numStructs = num;
+        externalNL = false;
         sfCap = 0;
         lastMaxNbr = 0;
         elemHost.assign(elems, elems + total);
@@ -793,6 +800,7 @@ struct n2p2b_context
                       int loc, int32_t const* elems, int flags)
     {
         numStructs = 0;
+        externalNL = false;
         graphValid = false;
         requireReady();
         if (num <= 0 || posArg == nullptr || elems == nullptr)
@@ -1023,6 +1031,7 @@ struct n2p2b_context
 
     void enqueueNL()
     {
+        if (externalNL) return;      // the caller's list is already in place
         if (numStructs > 0)
         {
             NLBatchLaunch B;
@@ -1749,7 +1758,140 @@ struct n2p2b_context
         L.F = F.as<double>();
         L.forceScale = pot.normalize ? pot.convEnergy / pot.convLength : 1.0;
         L.status = status.as<int>();
+        L.gather = externalNL ? 0 : 1;
         launchForces(L, stream);
+        if (!externalNL) return;
+        TargetForceLaunch T;
+        T.numLocal = (int)n;
+        T.numTargets = (int)numTargets;
+        T.revOff = revOff.as<int>();
+        T.revEntry = revEntry.as<int>();
+        T.selfF = selfF.as<double>();
+        T.pairF = pairF.as<double>();
+        T.F = Ftarget.as<double>();
+        T.forceScale = L.forceScale;
+        T.status = status.as<int>();
+        launchTargetForces(T, stream);
+    }
+
+    // ---- externally supplied neighbor list (InterfaceLammps path) ---------
+
+    // num local atoms (elements), each with counts[i] neighbors: the index
+    // of the neighbor in the caller's force array (local atoms first, then
+    // ghosts; numTargets in all), its element and r_i - r_neighbor in
+    // physical units.  Entries are regrouped by neighbor element (stable),
+    // as the symmetry-function kernel stages them.
+    void setNeighborList(long num, int32_t const* elems,
+                         int64_t const* counts, int64_t const* index,
+                         int32_t const* nelems, double const* drIn,
+                         long targets)
+    {
+        requireReady();
+        if (num <= 0 || !elems || !counts || targets < num)
+            throw std::invalid_argument("ERROR: Invalid neighbor list "
+                                        "arguments.\n");
+        int const ne = pot.numElements();
+        long E = 0;
+        for (long i = 0; i < num; ++i)
+        {
+            if (elems[i] < 0 || elems[i] >= ne || counts[i] < 0)
+                throw std::invalid_argument("ERROR: Bad atom in neighbor "
+                                            "list.\n");
+            E += counts[i];
+        }
+        if (E > 0 && (!index || !nelems || !drIn))
+            throw std::invalid_argument("ERROR: Missing neighbor arrays.\n");
+        if (E > 0x7ffffffeL || targets > 0x7ffffffeL)
+            throw std::invalid_argument("ERROR: Neighbor list too large.\n");
+        activate();
+        n = num;
+        numStructs = 0;
+        externalNL = true;
+        numTargets = targets;
+        graphValid = false;
+        elemHost.assign(elems, elems + num);
+        std::vector<int> byElem;
+        byElem.reserve(n);
+        std::memset(&es, 0, sizeof(es));
+        for (int e = 0; e < ne; ++e)
+        {
+            es.start[e] = (int)byElem.size();
+            for (long i = 0; i < n; ++i)
+                if (elemHost[i] == e) byElem.push_back((int)i);
+        }
+        es.start[ne] = (int)byElem.size();
+        for (int e = ne + 1; e <= kMaxElem; ++e) es.start[e] = es.start[ne];
+        double const L = pot.normalize ? pot.convLength : 1.0;
+        std::vector<int> off(n + 1, 0), cntE((std::size_t)n * ne, 0);
+        std::vector<int> idx(E), rev((std::size_t)targets + 1, 0);
+        std::vector<int8_t> el(E);
+        std::vector<double> x(E), y(E), z(E), d(E);
+        int maxCnt = 0;
+        long src = 0;
+        for (long i = 0; i < n; ++i)
+        {
+            off[i + 1] = off[i] + (int)counts[i];
+            maxCnt = std::max(maxCnt, (int)counts[i]);
+            long dst = off[i];
+            for (int e = 0; e < ne; ++e)
+                for (long k = src; k < src + counts[i]; ++k)
+                {
+                    if (nelems[k] < 0 || nelems[k] >= ne || index[k] < 0
+                        || index[k] >= targets)
+                        throw std::invalid_argument("ERROR: Bad neighbor "
+                                                    "entry.\n");
+                    if (nelems[k] != e) continue;
+                    double const a = drIn[3 * k], b = drIn[3 * k + 1],
+                                 c = drIn[3 * k + 2];
+                    idx[dst] = (int)index[k];
+                    el[dst] = (int8_t)e;
+                    // InterfaceLammps::addNeighbor: n.d = sqrt(d2), scaled
+                    // like the components.
+                    d[dst] = std::sqrt(a * a + b * b + c * c) * L;
+                    x[dst] = a * L;
+                    y[dst] = b * L;
+                    z[dst] = c * L;
+                    ++cntE[(std::size_t)i * ne + e];
+                    ++rev[idx[dst] + 1];
+                    ++dst;
+                }
+            src += counts[i];
+        }
+        for (long m = 0; m < targets; ++m) rev[m + 1] += rev[m];
+        std::vector<int> fill(rev.begin(), rev.end() - 1), revE(E);
+        for (long e = 0; e < E; ++e) revE[fill[idx[e]]++] = (int)e;
+        ensureStructureBuffers();
+        capacity = std::max(capacity, std::max(E, 1L));
+        ensureEntryBuffers();
+        elem.ensure(sizeof(int) * n);
+        atomsByElem.ensure(sizeof(int) * n);
+        revOff.ensure(sizeof(int) * (targets + 1));
+        revEntry.ensure(sizeof(int) * std::max(E, 1L));
+        Ftarget.ensure(sizeof(double) * 3 * targets);
+        auto up = [&](DevBuf& b, void const* h, std::size_t bytes) {
+            if (bytes)
+                ck(cudaMemcpyAsync(b.p, h, bytes, cudaMemcpyHostToDevice,
+                                   stream), "upload neighbor list");
+        };
+        up(elem, elemHost.data(), sizeof(int) * n);
+        up(atomsByElem, byElem.data(), sizeof(int) * n);
+        up(nbrOff, off.data(), sizeof(int) * (n + 1));
+        up(nbrCountElem, cntE.data(), sizeof(int) * cntE.size());
+        up(nbrIdx, idx.data(), sizeof(int) * E);
+        up(nbrEl, el.data(), E);
+        up(dx, x.data(), sizeof(double) * E);
+        up(dy, y.data(), sizeof(double) * E);
+        up(dz, z.data(), sizeof(double) * E);
+        up(dd, d.data(), sizeof(double) * E);
+        up(revOff, rev.data(), sizeof(int) * (targets + 1));
+        up(revEntry, revE.data(), sizeof(int) * E);
+        ck(cudaStreamSynchronize(stream), "neighbor list upload");
+        invalidate();
+        haveNL = true;
+        lastMaxNbr = maxCnt;
+        sfCap = 0;
+        fitSFCap(maxCnt);
+        applyTuned();
     }
 
     void checkLaunch(char const* what)
@@ -2062,6 +2204,9 @@ struct n2p2b_context
     // reference's list order (j ascending, then image).
     void refOrder(std::vector<int>& off, std::vector<long>& perm)
     {
+        if (externalNL)
+            throw StateError("ERROR: The neighbor list was supplied by the "
+                             "caller.\n");
         long const E = totalEntries();
         off.resize(n + 1);
         ck(cudaMemcpy(off.data(), nbrOff.p, sizeof(int) * (n + 1),
@@ -2430,6 +2575,29 @@ int n2p2b_setup(n2p2b_context* ctx, char const* directory)
         ctx, (d + "weights.%03zu.data").c_str());
 }
 
+double n2p2b_atomic_energy_offset(n2p2b_context const* ctx, int e)
+{
+    if (!ctx || e < 0 || e >= ctx->pot.numElements()) return 0.0;
+    return ctx->pot.elements[e].atomicEnergyOffset;
+}
+
+int n2p2b_atomic_number(n2p2b_context const* ctx, int e)
+{
+    if (!ctx || e < 0 || e >= ctx->pot.numElements()) return 0;
+    return ctx->pot.elements[e].atomicNumber;
+}
+
+int n2p2b_unit_conversion(n2p2b_context const* ctx, double* mean_energy,
+                          double* conv_energy, double* conv_length)
+{
+    if (!ctx) return 0;
+    bool const nz = ctx->pot.normalize;
+    if (mean_energy) *mean_energy = nz ? ctx->pot.meanEnergy : 0.0;
+    if (conv_energy) *conv_energy = nz ? ctx->pot.convEnergy : 1.0;
+    if (conv_length) *conv_length = nz ? ctx->pot.convLength : 1.0;
+    return nz ? 1 : 0;
+}
+
 int n2p2b_num_elements(n2p2b_context const* ctx)
 {
     return ctx ? ctx->pot.numElements() : 0;
@@ -2655,12 +2823,44 @@ int n2p2b_get_forces(n2p2b_context* ctx, double* forces, int location)
     return guarded(ctx, [&] {
         if (!ctx->haveF) throw StateError("ERROR: Forces not calculated.\n");
         if (!forces) throw std::invalid_argument("ERROR: forces");
+        if (ctx->externalNL)
+            throw StateError("ERROR: With a supplied neighbor list the forces "
+                             "are per target: n2p2b_get_target_forces.\n");
         ctx->activate();
         ck(cudaMemcpyAsync(forces, ctx->F.p, sizeof(double) * 3 * ctx->n,
                            location == N2P2B_DEVICE ? cudaMemcpyDeviceToDevice
                                                     : cudaMemcpyDeviceToHost,
                            ctx->stream), "read forces");
         ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+    });
+}
+
+int n2p2b_set_neighbor_list(n2p2b_context* ctx, int64_t num_atoms,
+                            int32_t const* elements,
+                            int64_t const* neighbor_counts,
+                            int64_t const* neighbor_index,
+                            int32_t const* neighbor_elements,
+                            double const* dr, int64_t num_targets)
+{
+    return guarded(ctx, [&] {
+        ctx->setNeighborList(num_atoms, elements, neighbor_counts,
+                             neighbor_index, neighbor_elements, dr,
+                             num_targets);
+    });
+}
+
+int n2p2b_get_target_forces(n2p2b_context* ctx, double* forces)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveF) throw StateError("ERROR: Forces not calculated.\n");
+        if (!ctx->externalNL)
+            throw StateError("ERROR: No supplied neighbor list.\n");
+        if (!forces) throw std::invalid_argument("ERROR: forces");
+        ctx->activate();
+        ck(cudaStreamSynchronize(ctx->stream), "synchronize");
+        ck(cudaMemcpy(forces, ctx->Ftarget.p,
+                      sizeof(double) * 3 * ctx->numTargets,
+                      cudaMemcpyDeviceToHost), "read forces");
     });
 }
 

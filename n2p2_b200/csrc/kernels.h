@@ -372,10 +372,30 @@ struct ForceLaunch
     double*        pairF = nullptr;   // [entries][3]
     double*        F = nullptr;       // [n][3] output (physical units)
     double         forceScale = 1.0;  // divide by (convEnergy / convLength)
+    int            gather = 1;        // 0: pair and self terms only
     int const*     status = nullptr;
 };
 
 void launchForces(ForceLaunch const& L, cudaStream_t s);
+
+// Forces for an externally supplied neighbor list (an MD engine's local and
+// ghost atoms, the InterfaceLammps::getForces scatter): thread per target
+// m, F_m = [m local] selfF_m + sum of pairF over the entries pointing to m
+// (revEntry[revOff[m] .. revOff[m + 1]), ascending: a fixed order).
+struct TargetForceLaunch
+{
+    int           numLocal = 0;
+    int           numTargets = 0;
+    int const*    revOff = nullptr;
+    int const*    revEntry = nullptr;
+    double const* selfF = nullptr;
+    double const* pairF = nullptr;
+    double*       F = nullptr;          // [numTargets][3]
+    double        forceScale = 1.0;
+    int const*    status = nullptr;
+};
+
+void launchTargetForces(TargetForceLaunch const& L, cudaStream_t s);
 
 struct EnergyLaunch
 {

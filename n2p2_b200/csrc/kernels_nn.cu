@@ -377,7 +377,39 @@ __global__ void energyBatchKernel(BatchEnergyLaunch const L)
     }
 }
 
+__global__ void targetForceKernel(TargetForceLaunch const L)
+{
+    int const m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= L.numTargets) return;
+    if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    if (m < L.numLocal)
+    {
+        fx = L.selfF[(long)m * 3 + 0];
+        fy = L.selfF[(long)m * 3 + 1];
+        fz = L.selfF[(long)m * 3 + 2];
+    }
+    for (int k = L.revOff[m]; k < L.revOff[m + 1]; ++k)
+    {
+        long const e = L.revEntry[k];
+        fx += L.pairF[e * 3 + 0];
+        fy += L.pairF[e * 3 + 1];
+        fz += L.pairF[e * 3 + 2];
+    }
+    L.F[(long)m * 3 + 0] = fx / L.forceScale;
+    L.F[(long)m * 3 + 1] = fy / L.forceScale;
+    L.F[(long)m * 3 + 2] = fz / L.forceScale;
+}
+
 } // namespace
+
+void launchTargetForces(TargetForceLaunch const& L, cudaStream_t s)
+{
+    int const tb = 128;
+    int const g = (L.numTargets + tb - 1) / tb;
+    noteLaunches(1);
+    targetForceKernel<<<g > 0 ? g : 1, tb, 0, s>>>(L);
+}
 
 void launchEnergyBatch(BatchEnergyLaunch const& L, cudaStream_t s)
 {
@@ -416,11 +448,12 @@ void launchForces(ForceLaunch const& L, cudaStream_t s)
     int const warps = 4;
     std::size_t const shm = sizeof(double) * warps * (std::size_t)L.maxSF;
     int const grid = (L.n + warps - 1) / warps;
-    noteLaunches(2);
+    noteLaunches(L.gather ? 2 : 1);
     if (L.precision != PREC_FP64)
         pairForceKernel<float><<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
     else
         pairForceKernel<double><<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
+    if (!L.gather) return;
     int const tb = 128;
     gatherForceKernel<<<(L.n + tb - 1) / tb > 0 ? (L.n + tb - 1) / tb : 1, tb,
                         0, s>>>(L);
