@@ -53,10 +53,12 @@ POT_DIR = os.path.join(ROOT, "tests", "golden", "potentials")
 POT = os.path.join(POT_DIR, "h2o_52")
 STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
-# DRAM bytes (read + write) of one symmetry-function launch on this
-# workload, from the ncu capture summarized under profiles/ (None until a
-# capture of the current kernel exists).
-SF_TRAFFIC_BYTES = None
+# DRAM bytes (read + write) of one FP64 symmetry-function launch on this
+# workload: the ncu capture summarized under profiles/ measured 1.058 GB on
+# the 12,288-atom box (DRAM throughput x duration); traffic grows with the
+# neighbor entries, i.e. with the atoms, so the 24,576-atom launch moves
+# twice that.
+SF_TRAFFIC_BYTES = 2.116e9
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
