@@ -483,6 +483,7 @@ struct n2p2b_context
             Element const& el = pot.elements[e];
             sfp.groupBeg[e] = gi;
             int expCount = 0;
+            std::vector<std::pair<double, double>> expKeys;
             sfp.numSF[e] = (int)el.sfs.size();
             for (int f = 0; f < ne; ++f)
             {
@@ -548,8 +549,20 @@ struct n2p2b_context
                             ? &el.sfs[g.members[k - 1]] : nullptr;
                         m.calcExp = (prev == nullptr || prev->eta != s.eta
                                      || prev->rs != s.rs) ? 1 : 0;
-                        if (m.calcExp) ++expCount;
-                        m.expIdx = (int16_t)(expCount - 1);
+                        // One exp(-eta (r - rs)^2) table per distinct
+                        // (eta, rs) of the element, shared by its groups.
+                        int idx = 0;
+                        while (idx < (int)expKeys.size()
+                               && !(expKeys[idx].first == s.eta
+                                    && expKeys[idx].second == s.rs))
+                            ++idx;
+                        if (idx == (int)expKeys.size())
+                        {
+                            expKeys.emplace_back(s.eta, s.rs);
+                            m.fillExp = 1;
+                        }
+                        expCount = (int)expKeys.size();
+                        m.expIdx = (int16_t)idx;
                         q.q = m.factorNorm / s.scalingFactor;
                     }
                     switch (s.scalingType)
@@ -1109,7 +1122,7 @@ struct n2p2b_context
             sfVariant = sfDefaultVariant(sfp);
             if (char const* v = std::getenv("N2P2B_SF_VARIANT"))
                 sfVariant = std::atoi(v);
-            sfSortCats = 1;
+            sfSortCats = 3;
             if (char const* v = std::getenv("N2P2B_SF_SORT"))
                 sfSortCats = std::atoi(v);
         }
@@ -2163,7 +2176,7 @@ struct n2p2b_context
         TuneChoice best{sfVariant, sfSortCats, nlWarpsPerBlock, t0};
         std::string rep;
         for (int v = 0; v < 4; ++v)
-            for (int so = 0; so < 2; ++so)
+            for (int so = 1; so <= 3; so += 2)
                 for (int w : nls)
                 {
                     sfVariant = v;

@@ -128,7 +128,8 @@ struct SFLaunch
     int            grid = 0;          // persistent grid size
     long           warpBytes = 0;     // shared memory per warp (set by launcher)
     int            variant = 0;       // product-form shape / run chunking
-    int            sortCats = 0;      // order work categories by partners
+    int            sortCats = 0;      // bit 0: order work categories by
+                                      // partners; bit 1: balanced owners
     int const*     elem = nullptr;
     int const*     nbrOff = nullptr;
     int const*     nbrCountElem = nullptr;

@@ -28,8 +28,8 @@ namespace
 long warpBytesFor(SFParams const& P, int cap, int precision)
 {
     return precision != PREC_FP64
-        ? sfk::warpBytes<float>(P.maxExp, P.maxSF, cap)
-        : sfk::warpBytes<double>(P.maxExp, P.maxSF, cap);
+        ? sfk::warpBytes<float>(P.maxExp, P.maxSF, cap, P.numElements)
+        : sfk::warpBytes<double>(P.maxExp, P.maxSF, cap, P.numElements);
 }
 
 } // namespace

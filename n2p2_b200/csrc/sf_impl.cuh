@@ -244,7 +244,15 @@ struct WarpMem
     R*        wpG;    // [maxSF]
     R*        wpS;    // [maxSF][3]
     struct Cat*  cats;  // work-item categories of the current segment
-    int          sortCats;  // order angular categories by partner count
+    int          sortCats;  // bit 0: order angular categories by partner
+                            // count; bit 1: balanced owner order
+    // The categories are followed (kCatsBytes further on) by the balanced
+    // owner order: the owners of each element ordered by their number of
+    // valid partners of element e2 (descending in 32 count buckets, ties by
+    // position), order[e2 * cap + t] for t in the owner element's range,
+    // then 32 ints of sort scratch.  The narrow angular paths walk owners
+    // in that order so that the 32 owners of a round have similar loop
+    // lengths.
 };
 
 // A category is a group together with one owner element: its items are the
@@ -252,22 +260,35 @@ struct WarpMem
 struct Cat
 {
     int gi, et, ob, on, pb, pe;
+    int oo;   // offset of the owners in the balanced order, -1: positions
 };
 // Segments hold at most kMaxSegGroups groups (longer runs of equal (type, rc)
 // are split), so the category table never overflows.
 constexpr int kMaxSegGroups = 16;
 constexpr int kMaxCats = 2 * kMaxSegGroups;
+constexpr long kCatsBytes = ((long)(kMaxCats * sizeof(Cat)) + 15) / 16 * 16;
+
+// The balanced owner order and its sort scratch (see WarpMem).
+template <typename R>
+__device__ __forceinline__ unsigned short* ownerOrder(WarpMem<R> const& W)
+{
+    return reinterpret_cast<unsigned short*>(
+        reinterpret_cast<char*>(W.cats) + kCatsBytes);
+}
 
 // Bytes of one warp's shared-memory region (16-byte multiple).
 template <typename R>
-__host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap)
+__host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap,
+                                          int numElements)
 {
     long const words = (cap + 31) / 32;
     long b = (long)sizeof(R) * (7L * cap + (long)maxExp * cap + 4L * maxSF);
     b = (b + 15) / 16 * 16;
     b += 4L * cap * words;                          // validity bits
     b = (b + 15) / 16 * 16;
-    b += (long)(kMaxCats * sizeof(Cat));            // categories
+    b += kCatsBytes;                                // categories
+    b += (2L * numElements * cap + 3) / 4 * 4;      // owner order
+    b += 4L * 32;                                   // count buckets
     return (b + 15) / 16 * 16;
 }
 
@@ -331,8 +352,8 @@ struct Item
 template <typename R>
 __device__ __forceinline__ int buildCats(DevGroup const* G, int g0, int g1,
                                          int const eb[kMaxElem + 1],
-                                         bool byPartners, WarpMem<R> const& W,
-                                         int& ncat)
+                                         bool byPartners, int orderCap,
+                                         WarpMem<R> const& W, int& ncat)
 {
     int const lane = threadIdx.x & 31;
     int n = 0, total = 0;
@@ -354,6 +375,7 @@ __device__ __forceinline__ int buildCats(DevGroup const* G, int g0, int g1,
                 c.on = eb[et + 1] - eb[et];
                 c.pb = eb[pe2];
                 c.pe = eb[pe2 + 1];
+                c.oo = orderCap > 0 ? pe2 * orderCap + c.ob : -1;
                 int pos = n;
                 if (byPartners)
                     while (pos > 0 && (W.cats[pos - 1].pe - W.cats[pos - 1].pb)
@@ -390,7 +412,7 @@ __device__ __forceinline__ Item itemOf(WarpMem<R> const& W, int ncat, int q)
         {
             it.gi = cc.gi;
             it.key = c;
-            it.t = cc.ob + q;
+            it.t = cc.oo >= 0 ? (int)ownerOrder(W)[cc.oo + q] : cc.ob + q;
             it.et = cc.et;
             it.pb = cc.pb;
             it.pe = cc.pe;
@@ -414,6 +436,68 @@ __device__ __forceinline__ unsigned rangeMask(unsigned m, int w, int pb, int pe)
     return m;
 }
 
+// Balanced owner order for owners [ob, oe) and partners [pb, pe): the owners
+// sorted by their number of valid partners, descending, by a stable warp
+// counting sort over 32 buckets of the count range (exact when the counts
+// span at most 32 values). Writes order[ob .. oe). Warp-uniform arguments.
+template <typename R>
+__device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
+                                int oe, int pb, int pe,
+                                unsigned short* __restrict__ order,
+                                int* __restrict__ hist)
+{
+    int const lane = threadIdx.x & 31;
+    if (oe <= ob) return;
+    auto count = [&](int t) {
+        int c = 0;
+        for (int w = pb >> 5; w < (pe + 31) >> 5; ++w)
+            c += __popc(rangeMask(W.bits[t * words + w], w, pb, pe));
+        return c;
+    };
+    int cmin = 0x7fffffff, cmax = 0;
+    for (int t = ob + lane; t < oe; t += 32)
+    {
+        int const c = count(t);
+        cmin = min(cmin, c);
+        cmax = max(cmax, c);
+    }
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        cmin = min(cmin, __shfl_xor_sync(kFull, cmin, o));
+        cmax = max(cmax, __shfl_xor_sync(kFull, cmax, o));
+    }
+    int const span = cmax - cmin + 1;
+    // Bucket 0 holds the owners with the most partners.
+    auto key = [&](int c) { return ((cmax - c) * 32) / span; };
+    hist[lane] = 0;
+    __syncwarp();
+    for (int t = ob + lane; t < oe; t += 32)
+        atomicAdd(&hist[key(count(t))], 1);
+    __syncwarp();
+    int const h = hist[lane];
+    int incl = h;
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int const v = __shfl_up_sync(kFull, incl, o);
+        if (lane >= o) incl += v;
+    }
+    __syncwarp();
+    hist[lane] = incl - h;
+    __syncwarp();
+    for (int t0 = ob; t0 < oe; t0 += 32)
+    {
+        int const t = t0 + lane;
+        bool const active = t < oe;
+        int const k = active ? key(count(t)) : 32 + lane;
+        unsigned const peers = __match_any_sync(kFull, k);
+        int const r = __popc(peers & ((1u << lane) - 1u));
+        if (active) order[ob + hist[k] + r] = (unsigned short)t;
+        __syncwarp();
+        if (active && r == 0) hist[k] += __popc(peers);
+        __syncwarp();
+    }
+}
+
 template <typename R, int MC>
 __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
                               int g1, int const eb[kMaxElem + 1], int cnt,
@@ -422,7 +506,7 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
-    int const items = buildCats(G, g0, g1, eb, false, W, ncat);
+    int const items = buildCats(G, g0, g1, eb, false, 0, W, ncat);
     int maxM = 0;
     for (int gi = g0; gi < g1; ++gi) maxM = max(maxM, G[gi].mcnt);
     for (int q0 = 0; q0 < items; q0 += 32)
@@ -478,7 +562,9 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
-    int const items = buildCats(G, g0, g1, eb, W.sortCats != 0, W, ncat);
+    int const items = buildCats(G, g0, g1, eb, (W.sortCats & 1) != 0,
+                                (NARROW && (W.sortCats & 2)) ? capE : 0, W,
+                                ncat);
     int maxM = 0;
     for (int gi = g0; gi < g1; ++gi) maxM = max(maxM, G[gi].mcnt);
     for (int q0 = 0; q0 < items; q0 += 32)
@@ -648,7 +734,9 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
-    int const items = buildCats(G, g0, g1, eb, W.sortCats != 0, W, ncat);
+    int const items = buildCats(G, g0, g1, eb, (W.sortCats & 1) != 0,
+                                (NARROW && (W.sortCats & 2)) ? capE : 0, W,
+                                ncat);
     int maxR = 0;
     for (int gi = g0; gi < g1; ++gi) maxR = max(maxR, G[gi].mcnt / NS);
     for (int q0 = 0; q0 < items; q0 += 32)
@@ -965,19 +1053,31 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                         W.bits[t * words + w] = m;
                     }
                 }
+                __syncwarp();
+                if (W.sortCats & 2)
+                {
+                    unsigned short* const order = ownerOrder(W);
+                    int* const hist = reinterpret_cast<int*>(
+                        order + (numElements * cap + 1) / 2 * 2);
+                    for (int e2 = 0; e2 < numElements; ++e2)
+                        for (int et = 0; et < numElements; ++et)
+                            buildOwnerOrder(W, words, eb[et], eb[et + 1],
+                                            eb[e2], eb[e2 + 1],
+                                            order + e2 * cap, hist);
+                }
                 bitsRc = h.rc;
             }
             if (h.type != 2)
             {
                 // Gaussian factors E(r) = exp(-eta (r - rs)^2) per distinct
-                // (eta, rs) run of the segment's members.
+                // (eta, rs) of the element (computed once per atom).
                 for (int gi = g0; gi < g1; ++gi)
                 {
                     DevGroup const& g = sG[gi];
                     for (int l = 0; l < g.mcnt; ++l)
                     {
                         DevMember const& mm = sM[g.mbeg + l];
-                        if (!mm.calcExp) continue;
+                        if (!mm.fillExp) continue;
                         R* E = W.E + (long)mm.expIdx * cap;
                         R const eta = R(mm.eta), rs = R(mm.rs);
                         for (int t = lane; t < cnt; t += 32)

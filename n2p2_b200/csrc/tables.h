@@ -43,7 +43,8 @@ struct DevMember
     uint8_t calcExp;      // first member of an (eta, rs) run
     uint8_t useIntPow;
     uint8_t rsPositive;
-    uint8_t pad;
+    uint8_t fillExp;      // first member of the element with its (eta, rs):
+                          // fills the atom's exp table expIdx
     int16_t slot[kMaxElem];  // dG/dr slot per neighbor element, -1 = none
     int16_t expIdx;       // per-element index of the member's (eta, rs) run
 };
@@ -54,7 +55,7 @@ struct SFParams
     int       cutoffType;      // CutoffType (global in n2p2)
     int       maxSlots;        // dG/dr slots per neighbor entry (stride)
     int       maxSF;           // SF stride of per-atom arrays
-    int       maxExp;          // max (eta, rs) runs of angular members/element
+    int       maxExp;          // distinct angular (eta, rs) per element, max
     int       groupBeg[kMaxElem + 1];
     int       numSF[kMaxElem];
     int       numSlots[kMaxElem][kMaxElem];
