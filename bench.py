@@ -54,11 +54,11 @@ POT = os.path.join(POT_DIR, "h2o_52")
 STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
 # DRAM bytes (read + write) of one FP64 symmetry-function launch on this
-# workload: the ncu capture summarized under profiles/ measured 1.058 GB on
-# the 12,288-atom box (DRAM throughput x duration); traffic grows with the
-# neighbor entries, i.e. with the atoms, so the 24,576-atom launch moves
-# twice that.
-SF_TRAFFIC_BYTES = 2.116e9
+# workload: the ncu capture summarized under profiles/ measured
+# dram__bytes_read.sum + dram__bytes_write.sum = 1.056 GB on the
+# 12,288-atom box; traffic grows with the neighbor entries, i.e. with the
+# atoms, so the 24,576-atom launch moves twice that.
+SF_TRAFFIC_BYTES = 2.112e9
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
@@ -375,12 +375,15 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
             forms += [("student_gated", "mixed", "gated"),
                       ("student_only", "mixed", "only")]
         refs = {}
+        tunes = {}
         for name, prec, smode in forms:
             p.set_precision(prec)
             if smode is not None:
                 p.set_student_mode(smode)
             p.set_positions(frames[0])
             p.evaluate_nnp(True)
+            if prec not in tunes:
+                tunes[prec] = p.autotune(True, 1)
             for s in range(3):
                 p.set_positions(dev_frames[s])
                 p.evaluate_async(True)
@@ -397,7 +400,8 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
             entry = {"value": n * steps / t, "unit": "atoms/s",
                      "ms_per_step": 1e3 * t / steps, "steps": steps,
                      "gpu_launches_per_step": launches / steps,
-                     "stage_ms_per_step": dict(zip(STAGES, stage))}
+                     "stage_ms_per_step": dict(zip(STAGES, stage)),
+                     "autotune": tunes[prec]}
             refs[name] = acc
             for rname in (("fp64", "mixed") if smode else ("fp64",)):
                 if name == rname:
@@ -534,6 +538,9 @@ def run_ours(a):
     p.set_stream(stream.cuda_stream)
     p.set_structure(host_frames[0].numpy(), elem, box)
     p.evaluate_nnp(True)          # sizes all buffers (capacity known)
+    # Launch configuration for this size bucket (Prediction.autotune, the
+    # library's own tuner; part of setup, outside the timed region).
+    tune = p.autotune(True, 1)
     lib = _capi.load()
 
     def barrier():
@@ -622,6 +629,7 @@ def run_ours(a):
                         "n2p2b_get_forces(host) + n2p2b_get_energy"},
         "gpu_launches": launches,
         "stage_ms_per_step": dict(zip(STAGES, per)),
+        "autotune": tune,
         "roofline": {"kernel": "sfKernel<double> (symmetry functions + "
                                "dG/dr)",
                      "bound": "hbm", "achieved": gbs, "peak": hbm_peak,

@@ -1122,7 +1122,7 @@ struct n2p2b_context
             sfVariant = sfDefaultVariant(sfp);
             if (char const* v = std::getenv("N2P2B_SF_VARIANT"))
                 sfVariant = std::atoi(v);
-            sfSortCats = 3;
+            sfSortCats = sfDefaultSort(sfp);
             if (char const* v = std::getenv("N2P2B_SF_SORT"))
                 sfSortCats = std::atoi(v);
         }
@@ -2131,7 +2131,14 @@ struct n2p2b_context
     void applyTuned()
     {
         auto it = tuned.find(tuneKey());
-        if (it == tuned.end()) return;
+        if (it == tuned.end())
+        {
+            // Untuned bucket: the defaults of the next launch.
+            sfVariant = -1;
+            sfGrid = 0;
+            graphValid = false;
+            return;
+        }
         sfVariant = it->second.variant;
         sfSortCats = it->second.sortCats;
         nlWarpsPerBlock = it->second.nlWarps;
@@ -2170,7 +2177,11 @@ struct n2p2b_context
             }
             return best;
         };
-        if (sfVariant < 0) sfVariant = sfDefaultVariant(sfp);
+        if (sfVariant < 0)
+        {
+            sfVariant = sfDefaultVariant(sfp);
+            sfSortCats = sfDefaultSort(sfp);
+        }
         TuneChoice const start{sfVariant, sfSortCats, nlWarpsPerBlock, 0.0};
         double const t0 = timeIt();
         TuneChoice best{sfVariant, sfSortCats, nlWarpsPerBlock, t0};

@@ -153,6 +153,10 @@ int sfAtomsPerBlock();
 // Kernel variant matching the potential's product-form groups:
 // 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
 int sfDefaultVariant(SFParams const& P);
+// Default SFLaunch::sortCats: the balanced owner order (bit 1) pays for its
+// per-atom sort when an element has many angular members (long per-pair
+// work); fewer members keep positional order.
+int sfDefaultSort(SFParams const& P);
 
 // Atomic neural networks (forward + dE/dG) on the SIMT cores: FP64 (plain
 // form) or FP32 (precision != PREC_FP64: the distilled student network).

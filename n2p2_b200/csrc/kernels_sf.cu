@@ -2,6 +2,8 @@
 // and dispatch to the kernel instantiated for the potential's cutoff type and
 // the context's precision (kernels_sf_{cos,tanhu,poly2,any}{,_f32}.cu,
 // templates in sf_impl.cuh).
+#include <algorithm>
+
 #include "kernels.h"
 #include "sf_impl.cuh"
 
@@ -69,6 +71,19 @@ int sfDefaultVariant(SFParams const& P)
         if (P.groups[g].shapes == 8) ++n8;
     }
     return (n8 > n4) ? 2 : 0;
+}
+
+int sfDefaultSort(SFParams const& P)
+{
+    int most = 0;
+    for (int e = 0; e < P.numElements; ++e)
+    {
+        int m = 0;
+        for (int g = P.groupBeg[e]; g < P.groupBeg[e + 1]; ++g)
+            if (P.groups[g].type != 2) m += P.groups[g].mcnt;
+        most = std::max(most, m);
+    }
+    return most >= 64 ? 3 : 1;
 }
 
 void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,

@@ -2,13 +2,18 @@
 
     python -m n2p2_b200.profile_case [--molecules 4096] [--potential h2o_52]
                                      [--precision fp64|mixed|bf16]
-                                     [--evaluations 5]
+                                     [--evaluations 5] [--autotune]
 
 Builds a seeded water box (seed 77), sets it on a Prediction of one of the
 test potentials, evaluates `--evaluations` times (energy + forces) and
 prints the per-stage device times of the last three evaluations.  The
 symmetry-function kernel of evaluation k is launch k of that kernel (after
 the first evaluation's sizing pass, which launches the neighbor list only).
+
+`--autotune` runs the library's tuner (Prediction.autotune) first and
+prints its choice; the tuner launches every configuration, so a capture
+that should see launch k takes the printed choice through the
+N2P2B_SF_VARIANT / N2P2B_SF_SORT environment variables instead.
 """
 from __future__ import annotations
 
@@ -29,6 +34,7 @@ def main():
     a.add_argument("--precision", default="fp64",
                    choices=["fp64", "mixed", "bf16"])
     a.add_argument("--evaluations", type=int, default=5)
+    a.add_argument("--autotune", action="store_true")
     args = a.parse_args()
     box, pos, elem = synth.water_box(args.molecules, 77)
     p = Prediction(os.path.join(POTENTIALS, args.potential))
@@ -36,6 +42,9 @@ def main():
     p.setup_symmetry_function_statistics(False, False, False, False)
     p.set_precision(args.precision)
     p.set_structure(pos, elem, box)
+    if args.autotune:
+        p.evaluate_nnp(True)
+        print("autotune", p.autotune(True, 3))
     for _ in range(max(args.evaluations - 3, 1)):
         p.evaluate_nnp(True)
     p.set_profiling(True)
