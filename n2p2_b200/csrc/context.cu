@@ -941,7 +941,6 @@ struct n2p2b_context
         nbrOff.ensure(sizeof(int) * (n + 1));
         G.ensure(realBytes() * n * maxSF);
         dEdG.ensure(realBytes() * n * maxSF);
-        dGdrSelf.ensure(realBytes() * n * maxSF * 3);
         Ei.ensure(sizeof(double) * n);
         ewPerAtom.ensure(sizeof(int) * n);
         if (stu.loaded) stu.list.ensure(sizeof(int) * n);
@@ -1153,7 +1152,6 @@ struct n2p2b_context
         L.scale = sfScale.as<SFScale>();
         L.precision = precision;
         L.G = G.p;
-        L.dGdrSelf = dGdrSelf.p;
         L.dGdr = dGdr.p;
         L.status = status.as<int>();
         launchSymmetryFunctions(sfp, L, stream);
@@ -1523,7 +1521,6 @@ struct n2p2b_context
         stu.gpart.ensure(sizeof(float) * std::max(blocks, 1)
                          * (std::size_t)stu.maxParams);
         S.G = G.p;
-        S.dGdrSelf = dGdrSelf.p;
         S.dGdr = dGdr.p;
         S.Ei = Ei.as<double>();
         S.F = F.as<double>();
@@ -1743,7 +1740,37 @@ struct n2p2b_context
         launchEnergy(L, stream);
     }
 
+    // dG/dr (self) of every atom into dGdrSelf, formed from the stored
+    // neighbor slots (the evaluation path never needs it on its own).
+    void formSelfDerivatives()
+    {
+        dGdrSelf.ensure(realBytes() * n * maxSF * 3);
+        ForceLaunch L = forceLaunch();
+        launchSelfDerivatives(L, dGdrSelf.p, stream);
+        checkLaunch("self derivatives");
+        ck(cudaStreamSynchronize(stream), "synchronize");
+    }
+
     void enqueueForces()
+    {
+        ForceLaunch L = forceLaunch();
+        L.gather = externalNL ? 0 : 1;
+        launchForces(L, stream);
+        if (!externalNL) return;
+        TargetForceLaunch T;
+        T.numLocal = (int)n;
+        T.numTargets = (int)numTargets;
+        T.revOff = revOff.as<int>();
+        T.revEntry = revEntry.as<int>();
+        T.selfF = selfF.as<double>();
+        T.pairF = pairF.as<double>();
+        T.F = Ftarget.as<double>();
+        T.forceScale = L.forceScale;
+        T.status = status.as<int>();
+        launchTargetForces(T, stream);
+    }
+
+    ForceLaunch forceLaunch()
     {
         ForceLaunch L;
         int const ne = pot.numElements();
@@ -1764,27 +1791,13 @@ struct n2p2b_context
         }
         L.precision = precision;
         L.dEdG = dEdG.p;
-        L.dGdrSelf = dGdrSelf.p;
         L.dGdr = dGdr.p;
         L.selfF = selfF.as<double>();
         L.pairF = pairF.as<double>();
         L.F = F.as<double>();
         L.forceScale = pot.normalize ? pot.convEnergy / pot.convLength : 1.0;
         L.status = status.as<int>();
-        L.gather = externalNL ? 0 : 1;
-        launchForces(L, stream);
-        if (!externalNL) return;
-        TargetForceLaunch T;
-        T.numLocal = (int)n;
-        T.numTargets = (int)numTargets;
-        T.revOff = revOff.as<int>();
-        T.revEntry = revEntry.as<int>();
-        T.selfF = selfF.as<double>();
-        T.pairF = pairF.as<double>();
-        T.F = Ftarget.as<double>();
-        T.forceScale = L.forceScale;
-        T.status = status.as<int>();
-        launchTargetForces(T, stream);
+        return L;
     }
 
     // ---- externally supplied neighbor list (InterfaceLammps path) ---------
@@ -3002,6 +3015,7 @@ int n2p2b_get_dGdr(n2p2b_context* ctx, double* self, int sfStride,
         int const S = ctx->maxSlots;
         if (self)
         {
+            ctx->formSelfDerivatives();
             std::vector<double> const g =
                 ctx->readReal(ctx->dGdrSelf, (std::size_t)n * ctx->maxSF * 3);
             for (long i = 0; i < n; ++i)

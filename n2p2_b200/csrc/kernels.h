@@ -140,7 +140,6 @@ struct SFLaunch
     SFScale const* scale = nullptr;   // [element][maxSF]
     // Outputs in the compute type (double, or float in the mixed form).
     void*          G = nullptr;       // [n][maxSF]
-    void*          dGdrSelf = nullptr;// [n][maxSF][3]
     void*          dGdr = nullptr;    // per atom block [slot][3][neighbors]
     int*           status = nullptr;
 };
@@ -309,7 +308,6 @@ struct StudentLaunch
     ElemStarts     es{};
     int            blkBeg[kMaxElem + 1] = {}; // gradient blocks per element
     void const*    G = nullptr;
-    void const*    dGdrSelf = nullptr;
     void const*    dGdr = nullptr;
     double const*  Ei = nullptr;              // student atomic energies
     double const*  F = nullptr;               // student forces [n][3]
@@ -371,7 +369,6 @@ struct ForceLaunch
     int            numSlots[kMaxElem][kMaxElem] = {};
     int            precision = PREC_FP64;  // type of the three inputs below
     void const*    dEdG = nullptr;
-    void const*    dGdrSelf = nullptr;
     void const*    dGdr = nullptr;
     double*        selfF = nullptr;   // [n][3]
     double*        pairF = nullptr;   // [entries][3]
@@ -382,6 +379,11 @@ struct ForceLaunch
 };
 
 void launchForces(ForceLaunch const& L, cudaStream_t s);
+// dG/dr_i (self) of every atom into out [n][maxSF][3] (type of dGdr):
+// minus the sum of its neighbor slots, per neighbor element in entry order
+// (Atom::dGdr up to summation order).  Uses L's neighbor-list, slot-table
+// and dGdr fields; not on the evaluation path.
+void launchSelfDerivatives(ForceLaunch const& L, void* out, cudaStream_t s);
 
 // Forces for an externally supplied neighbor list (an MD engine's local and
 // ghost atoms, the InterfaceLammps::getForces scatter): thread per target

@@ -15,7 +15,10 @@
 // those entries are exactly the mirrors of i's own entries (i -> j, bc), so:
 //   pass 1 (warp per owner atom j, lanes over its entries, coalesced reads
 //           of the stored dG/dr):  pairF[e] = -sum_s dEdG_j[table(s)] dGdr[e][s]
-//           and selfF[j] = -sum_s dEdG_j[s] dGdr_self[j][s];
+//           and selfF[j] = -sum_s dEdG_j[s] dGdr_self[j][s] = -sum_e pairF[e]
+//           (the reference's self derivative is minus the sum of the
+//           neighbor slots: SymGrpExpRad.cpp:215-226,
+//           SymGrpExpAngn.cpp:366-383);
 //   pass 2 (thread per atom i): F_i = selfF_i + sum over i's entries e with
 //           index != i of pairF[mirror[e]]
 // -- a fixed-order segmented reduction, no atomics.  Entries of i pointing to
@@ -238,10 +241,13 @@ pairForceKernel(ForceLaunch const L)
     int const lane = threadIdx.x & 31;
     int const w = threadIdx.x >> 5;
     int const warps = blockDim.x >> 5;
-    double* dE = smem + (long)w * L.maxSF;
+    int const S = L.maxSlots;
+    // dE/dG of the owner, then its coefficients per (neighbor element, slot)
+    // so the entry loop reads one shared word per slot.
+    double* dE = smem + (long)w * (L.maxSF + L.numElements * S);
+    double* cE = dE + L.maxSF;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
     T const* const dEdG = static_cast<T const*>(L.dEdG);
-    T const* const dGdrSelf = static_cast<T const*>(L.dGdrSelf);
     T const* const dGdr = static_cast<T const*>(L.dGdr);
     for (int j = blockIdx.x * warps + w; j < L.n; j += gridDim.x * warps)
     {
@@ -249,15 +255,38 @@ pairForceKernel(ForceLaunch const L)
         T const* src = dEdG + (long)j * L.maxSF;
         for (int s = lane; s < L.maxSF; s += 32) dE[s] = (double)src[s];
         __syncwarp();
-        // Self force.
-        double fx = 0.0, fy = 0.0, fz = 0.0;
-        T const* gs = dGdrSelf + (long)j * L.maxSF * 3;
-        int const numSF = L.numSF[ej];
-        for (int s = lane; s < numSF; s += 32)
+        for (int k = lane; k < L.numElements * S; k += 32)
         {
-            fx -= dE[s] * (double)gs[s * 3 + 0];
-            fy -= dE[s] * (double)gs[s * 3 + 1];
-            fz -= dE[s] * (double)gs[s * 3 + 2];
+            int const en = k / S, s = k - en * S;
+            cE[k] = s < L.numSlots[ej][en]
+                  ? dE[L.slotSF[((long)ej * kMaxElem + en) * S + s]] : 0.0;
+        }
+        __syncwarp();
+        // Pair terms of j's entries; the self force is minus their sum.
+        double fx = 0.0, fy = 0.0, fz = 0.0;
+        long const b = L.nbrOff[j];
+        int const cnt = L.nbrOff[j + 1] - (int)b;
+        T const* gd = dGdr + b * (long)S * 3;
+        for (int t = lane; t < cnt; t += 32)
+        {
+            int const en = L.nbrEl[b + t];
+            int const ns = L.numSlots[ej][en];
+            double const* c = cE + en * S;
+            double px = 0.0, py = 0.0, pz = 0.0;
+#pragma unroll 4
+            for (int s = 0; s < ns; ++s)
+            {
+                T const* g = gd + (long)s * 3 * cnt + t;
+                px -= c[s] * (double)g[0];
+                py -= c[s] * (double)g[cnt];
+                pz -= c[s] * (double)g[2 * cnt];
+            }
+            L.pairF[(b + t) * 3 + 0] = px;
+            L.pairF[(b + t) * 3 + 1] = py;
+            L.pairF[(b + t) * 3 + 2] = pz;
+            fx -= px;
+            fy -= py;
+            fz -= pz;
         }
         fx = warpSum(fx);
         fy = warpSum(fy);
@@ -268,28 +297,48 @@ pairForceKernel(ForceLaunch const L)
             L.selfF[(long)j * 3 + 1] = fy;
             L.selfF[(long)j * 3 + 2] = fz;
         }
-        // Pair terms of j's entries.
+        __syncwarp();
+    }
+}
+
+// Warp per atom j: dG/dr_j (self) = -sum over j's entries of the slots,
+// neighbor element by neighbor element, lanes over entries.
+template <typename T>
+__global__ void __launch_bounds__(128)
+selfDerivativeKernel(ForceLaunch const L, T* __restrict__ out)
+{
+    extern __shared__ double acc0[];
+    int const lane = threadIdx.x & 31;
+    int const w = threadIdx.x >> 5;
+    int const warps = blockDim.x >> 5;
+    double* acc = acc0 + (long)w * L.maxSF * 3;
+    T const* const dGdr = static_cast<T const*>(L.dGdr);
+    for (int j = blockIdx.x * warps + w; j < L.n; j += gridDim.x * warps)
+    {
+        int const ej = L.elem[j];
+        for (int k = lane; k < L.maxSF * 3; k += 32) acc[k] = 0.0;
+        __syncwarp();
         long const b = L.nbrOff[j];
         int const cnt = L.nbrOff[j + 1] - (int)b;
         T const* gd = dGdr + b * (long)L.maxSlots * 3;
-        for (int t = lane; t < cnt; t += 32)
+        for (int en = 0; en < L.numElements; ++en)
         {
-            int const en = L.nbrEl[b + t];
-            int const ns = L.numSlots[ej][en];
             int16_t const* tab = L.slotSF + ((long)ej * kMaxElem + en)
                                             * L.maxSlots;
-            double px = 0.0, py = 0.0, pz = 0.0;
-            for (int s = 0; s < ns; ++s)
-            {
-                double const c = dE[tab[s]];
-                px -= c * (double)gd[((long)s * 3 + 0) * cnt + t];
-                py -= c * (double)gd[((long)s * 3 + 1) * cnt + t];
-                pz -= c * (double)gd[((long)s * 3 + 2) * cnt + t];
-            }
-            L.pairF[(b + t) * 3 + 0] = px;
-            L.pairF[(b + t) * 3 + 1] = py;
-            L.pairF[(b + t) * 3 + 2] = pz;
+            for (int sl = 0; sl < L.numSlots[ej][en]; ++sl)
+                for (int c = 0; c < 3; ++c)
+                {
+                    double v = 0.0;
+                    for (int t = lane; t < cnt; t += 32)
+                        if (L.nbrEl[b + t] == en)
+                            v += (double)gd[((long)sl * 3 + c) * cnt + t];
+                    v = warpSum(v);
+                    if (lane == 0) acc[tab[sl] * 3 + c] -= v;
+                    __syncwarp();
+                }
         }
+        for (int k = lane; k < L.maxSF * 3; k += 32)
+            out[(long)j * L.maxSF * 3 + k] = (T)acc[k];
         __syncwarp();
     }
 }
@@ -446,7 +495,8 @@ void launchNeuralNetworks(NNParams const& P, NNLaunch const& L,
 void launchForces(ForceLaunch const& L, cudaStream_t s)
 {
     int const warps = 4;
-    std::size_t const shm = sizeof(double) * warps * (std::size_t)L.maxSF;
+    std::size_t const shm = sizeof(double) * warps
+                          * (std::size_t)(L.maxSF + L.numElements * L.maxSlots);
     int const grid = (L.n + warps - 1) / warps;
     noteLaunches(L.gather ? 2 : 1);
     if (L.precision != PREC_FP64)
@@ -457,6 +507,20 @@ void launchForces(ForceLaunch const& L, cudaStream_t s)
     int const tb = 128;
     gatherForceKernel<<<(L.n + tb - 1) / tb > 0 ? (L.n + tb - 1) / tb : 1, tb,
                         0, s>>>(L);
+}
+
+void launchSelfDerivatives(ForceLaunch const& L, void* out, cudaStream_t s)
+{
+    int const warps = 4;
+    std::size_t const shm = sizeof(double) * warps * 3 * (std::size_t)L.maxSF;
+    int const grid = (L.n + warps - 1) / warps;
+    noteLaunches(1);
+    if (L.precision != PREC_FP64)
+        selfDerivativeKernel<float><<<grid > 0 ? grid : 1, 32 * warps, shm,
+                                      s>>>(L, static_cast<float*>(out));
+    else
+        selfDerivativeKernel<double><<<grid > 0 ? grid : 1, 32 * warps, shm,
+                                       s>>>(L, static_cast<double*>(out));
 }
 
 void launchEnergy(EnergyLaunch const& L, cudaStream_t s)

@@ -11,7 +11,9 @@
 //
 // The force term's gradient needs, for every atom j near the batch, the
 // adjoint u_js = -2 wF / (3|B|) sum_{i in B} r_i . dG_js/dr_i (r_i the force
-// residual), after which
+// residual; with dG_j/dr_j = -sum over j's entries of the neighbor slots,
+// u_js = -2 wF / (3|B|) sum_e (r_i(e) - r_j) . slot_e, r_i(e) = 0 for
+// entries that are images of j itself), after which
 //   d loss / d theta = sum_j [ c_j dE_j/d theta + d (u_j . dE_j/dG_j) / d theta ],
 //   c_j = 2 wE / |B| (E_j - E_j^T) for j in B, else 0.
 // With h = tanh(z), t = 1 - h^2 and a = W1 u_j the second term is
@@ -68,7 +70,6 @@ adjointKernel(StudentLaunch const L)
     int const w = threadIdx.x >> 5;
     int const warps = blockDim.x >> 5;
     float* acc = usm + (long)w * L.maxSF;
-    T const* const self = static_cast<T const*>(L.dGdrSelf);
     T const* const nbr = static_cast<T const*>(L.dGdr);
     float const scale = (float)(-2.0 * L.wF * L.fScale
                                 / (3.0 * L.batchSize));
@@ -79,11 +80,7 @@ adjointKernel(StudentLaunch const L)
         float const rx = L.rF[(long)j * 3 + 0];
         float const ry = L.rF[(long)j * 3 + 1];
         float const rz = L.rF[(long)j * 3 + 2];
-        for (int s = lane; s < nsf; s += 32)
-        {
-            T const* g = self + ((long)j * L.maxSF + s) * 3;
-            acc[s] = rx * (float)g[0] + ry * (float)g[1] + rz * (float)g[2];
-        }
+        for (int s = lane; s < nsf; s += 32) acc[s] = 0.0f;
         __syncwarp();
         long const b = L.nbrOff[j];
         int const cnt = L.nbrOff[j + 1] - (int)b;
@@ -103,13 +100,18 @@ adjointKernel(StudentLaunch const L)
                 for (int t = sb + lane; t < se; t += 32)
                 {
                     int const i = L.nbrIdx[b + t];
-                    if (i == j) continue;   // periodic self image: no force
-                    v += L.rF[(long)i * 3 + 0]
-                           * (float)gd[((long)sl * 3 + 0) * cnt + t]
-                       + L.rF[(long)i * 3 + 1]
-                           * (float)gd[((long)sl * 3 + 1) * cnt + t]
-                       + L.rF[(long)i * 3 + 2]
-                           * (float)gd[((long)sl * 3 + 2) * cnt + t];
+                    // A periodic self image carries no pair force, only its
+                    // share of j's self derivative.
+                    float qx = -rx, qy = -ry, qz = -rz;
+                    if (i != j)
+                    {
+                        qx += L.rF[(long)i * 3 + 0];
+                        qy += L.rF[(long)i * 3 + 1];
+                        qz += L.rF[(long)i * 3 + 2];
+                    }
+                    v += qx * (float)gd[((long)sl * 3 + 0) * cnt + t]
+                       + qy * (float)gd[((long)sl * 3 + 1) * cnt + t]
+                       + qz * (float)gd[((long)sl * 3 + 2) * cnt + t];
                 }
                 v = warpSumF(v);
                 if (lane == 0) acc[tab[sl]] += v;

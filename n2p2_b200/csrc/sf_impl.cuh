@@ -23,9 +23,15 @@
 // of the group's other element,
 //   * its own dG/dr slot:  -(sum_k p1(j,k)) dr_ij - sum_k p3(j,k) (dr_ik - dr_ij)
 //     -- kept in registers and written once (single writer, no atomics);
-//   * the self derivative sum_k p1(j,k) dr_ij and the value 1/2 sum_k term(j,k)
-//     (each unordered pair is seen by both owners; 0.5 scales exactly),
-//     folded into per-warp sums keyed by symmetry function.
+//   * the value 1/2 sum_k term(j,k) (each unordered pair is seen by both
+//     owners; 0.5 scales exactly), folded into per-warp sums keyed by
+//     symmetry function.
+// The self derivative dG/dr_i is not formed: the reference adds to the atom
+// exactly what it subtracts from the neighbor slots
+// (SymGrpExpRad.cpp:215-226, SymGrpExpAngn.cpp:366-383), so
+// dG/dr_i = -sum over entries of the slots, which the force kernel applies
+// as minus the sum of the atom's pair terms (and selfDerivativeKernel forms
+// on request).
 // For j as first member of the pair p1 is the reference's p1, for j as second
 // it is the reference's p2 -- the same expression with roles swapped.
 // Narrow-angular partners come from a per-atom validity bitmask
@@ -242,7 +248,6 @@ struct WarpMem
     R*        E;      // [expIdx][cap]
     unsigned* bits;   // [owner][words]
     R*        wpG;    // [maxSF]
-    R*        wpS;    // [maxSF][3]
     struct Cat*  cats;  // work-item categories of the current segment
     int          sortCats;  // bit 0: order angular categories by partner
                             // count; bit 1: balanced owner order
@@ -282,7 +287,7 @@ __host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap,
                                           int numElements)
 {
     long const words = (cap + 31) / 32;
-    long b = (long)sizeof(R) * (7L * cap + (long)maxExp * cap + 4L * maxSF);
+    long b = (long)sizeof(R) * (7L * cap + (long)maxExp * cap + maxSF);
     b = (b + 15) / 16 * 16;
     b += 4L * cap * words;                          // validity bits
     b = (b + 15) / 16 * 16;
@@ -292,7 +297,7 @@ __host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap,
     return (b + 15) / 16 * 16;
 }
 
-// Adds each lane's (G, self) contribution for symmetry function `sf` (-1 =
+// Adds each lane's G contribution for symmetry function `sf` (-1 =
 // nothing) into the warp sums.  `key` identifies the lane's work-item
 // category; lanes of one category occupy contiguous lanes (items are
 // enumerated category by category).  One segmented butterfly reduces every
@@ -300,37 +305,22 @@ __host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap,
 // totals one after another (two runs may share sf).
 template <typename R>
 __device__ __forceinline__ void flushBySF(WarpMem<R> const& W, int key, int sf,
-                                          R g, R sx, R sy, R sz)
+                                          R g)
 {
     int const lane = threadIdx.x & 31;
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1)
     {
         R const a = __shfl_down_sync(kFull, g, off);
-        R const b = __shfl_down_sync(kFull, sx, off);
-        R const c = __shfl_down_sync(kFull, sy, off);
-        R const e = __shfl_down_sync(kFull, sz, off);
         int const ko = __shfl_down_sync(kFull, key, off);
-        if (lane + off < 32 && ko == key)
-        {
-            g += a;
-            sx += b;
-            sy += c;
-            sz += e;
-        }
+        if (lane + off < 32 && ko == key) g += a;
     }
     int const prev = __shfl_up_sync(kFull, key, 1);
     bool const head = (lane == 0) || (prev != key);
     unsigned heads = __ballot_sync(kFull, head && sf >= 0);
     while (heads)
     {
-        if (lane == __ffs(heads) - 1)
-        {
-            W.wpG[sf] += g;
-            W.wpS[3 * sf + 0] += sx;
-            W.wpS[3 * sf + 1] += sy;
-            W.wpS[3 * sf + 2] += sz;
-        }
+        if (lane == __ffs(heads) - 1) W.wpG[sf] += g;
         __syncwarp();
         heads &= heads - 1;
     }
@@ -546,7 +536,7 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
                     out[(s * 3 + 1) * cnt + t] = -sy;
                     out[(s * 3 + 2) * cnt + t] = -sz;
                 }
-                flushBySF(W, it.key, has ? (int)m.sf : -1, gs, sx, sy, sz);
+                flushBySF(W, it.key, has ? (int)m.sf : -1, gs);
             }
         }
     }
@@ -716,8 +706,7 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                     out[(s * 3 + 1) * cnt + t] = -(sy + aPy[l]);
                     out[(s * 3 + 2) * cnt + t] = -(sz + aPz[l]);
                 }
-                flushBySF(W, it.key, has ? (int)mm.sf : -1, R(0.5) * aG[l],
-                          sx, sy, sz);
+                flushBySF(W, it.key, has ? (int)mm.sf : -1, R(0.5) * aG[l]);
             }
         }
     }
@@ -889,7 +878,7 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                         out[(sl * 3 + 2) * cnt + t] = -(sz + fn * aPz[r][s]);
                     }
                     flushBySF(W, it.key, has ? (int)mm.sf : -1,
-                              R(0.5) * aG[r][s], sx, sy, sz);
+                              R(0.5) * aG[r][s]);
                 }
         }
     }
@@ -910,8 +899,11 @@ inline int L_pathsOverride()
 constexpr int kPathRadial = 1, kPathFastNarrow = 2, kPathFastWide = 4,
               kPathGenNarrow = 8, kPathGenWide = 16, kPathAll = 31;
 
+// FP32 with up to 12 members per register chunk: at most 168 registers, so
+// that three CTAs (12 warps) fit per SM.
 template <typename R, int CT, int NS, int NRC, int PATHS>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads,
+                                  (sizeof(R) == 4 && NS * NRC <= 12) ? 3 : 1)
 sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 {
     extern __shared__ double smem0[];
@@ -954,9 +946,8 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     W.dfcr = W.fc + cap;
     W.E = W.dfcr + cap;
     W.wpG = W.E + (long)P.maxExp * cap;
-    W.wpS = W.wpG + maxSF;
     {
-        char* after = reinterpret_cast<char*>(W.wpS + 3 * maxSF);
+        char* after = reinterpret_cast<char*>(W.wpG + maxSF);
         long const off = (after - reinterpret_cast<char*>(wbase) + 15) / 16
                        * 16;
         W.bits = reinterpret_cast<unsigned*>(
@@ -966,7 +957,6 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     }
     W.sortCats = L.sortCats;
     R* const outG = static_cast<R*>(L.G);
-    R* const outSelf = static_cast<R*>(L.dGdrSelf);
     R* const outNbr = static_cast<R*>(L.dGdr);
 
     int const numElements = P.numElements;
@@ -1000,7 +990,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             W.d[t] = R(dd);
             W.inv[t] = R(1.0 / dd);
         }
-        for (int k = lane; k < 4 * maxSF; k += 32) W.wpG[k] = R(0);
+        for (int k = lane; k < maxSF; k += 32) W.wpG[k] = R(0);
         __syncwarp();
         R* out = outNbr + beg * (long)P.maxSlots * 3;
         double fcRc = -1.0;
@@ -1144,13 +1134,6 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             SFScale const q = sc[s];
             outG[(long)i * maxSF + s] =
                 R(q.smin + q.b * (q.q * (double)W.wpG[s] - q.shift));
-            if (L.derivatives)
-            {
-                R* o = outSelf + ((long)i * maxSF + s) * 3;
-                o[0] = W.wpS[3 * s + 0];
-                o[1] = W.wpS[3 * s + 1];
-                o[2] = W.wpS[3 * s + 2];
-            }
         }
         __syncwarp();
     }
