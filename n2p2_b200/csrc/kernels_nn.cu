@@ -34,6 +34,8 @@ namespace
 {
 
 constexpr int kNNWarps = 4;
+constexpr int kPairChunks = 4;      // entries per lane in one pair-force block
+constexpr int kPairAhead = 4;       // slots prefetched ahead into L2
 constexpr double kExpLimit = 35.0;  // EXP_LIMIT, libnnp/NeuralNetwork.cpp:25
 
 // Activation value and derivative (NeuralNetwork::propagateLayer).
@@ -263,30 +265,73 @@ pairForceKernel(ForceLaunch const L)
         }
         __syncwarp();
         // Pair terms of j's entries; the self force is minus their sum.
+        // Blocks of 32 * kPairChunks entries, slot loop outermost: the warp
+        // reads each (slot, component) row of the block as one contiguous
+        // run, so no DRAM sector is fetched twice.
         double fx = 0.0, fy = 0.0, fz = 0.0;
         long const b = L.nbrOff[j];
         int const cnt = L.nbrOff[j + 1] - (int)b;
         T const* gd = dGdr + b * (long)S * 3;
-        for (int t = lane; t < cnt; t += 32)
+        int smax = 0;
+        for (int en = 0; en < L.numElements; ++en)
+            smax = max(smax, L.numSlots[ej][en]);
+        for (int t0 = 0; t0 < cnt; t0 += 32 * kPairChunks)
         {
-            int const en = L.nbrEl[b + t];
-            int const ns = L.numSlots[ej][en];
-            double const* c = cE + en * S;
-            double px = 0.0, py = 0.0, pz = 0.0;
-#pragma unroll 4
-            for (int s = 0; s < ns; ++s)
+            double px[kPairChunks], py[kPairChunks], pz[kPairChunks];
+            int ns[kPairChunks], eo[kPairChunks];
+#pragma unroll
+            for (int k = 0; k < kPairChunks; ++k)
             {
-                T const* g = gd + (long)s * 3 * cnt + t;
-                px -= c[s] * (double)g[0];
-                py -= c[s] * (double)g[cnt];
-                pz -= c[s] * (double)g[2 * cnt];
+                int const t = t0 + 32 * k + lane;
+                int const en = t < cnt ? L.nbrEl[b + t] : 0;
+                ns[k] = t < cnt ? L.numSlots[ej][en] : 0;
+                eo[k] = en * S;
+                px[k] = py[k] = pz[k] = 0.0;
             }
-            L.pairF[(b + t) * 3 + 0] = px;
-            L.pairF[(b + t) * 3 + 1] = py;
-            L.pairF[(b + t) * 3 + 2] = pz;
-            fx -= px;
-            fy -= py;
-            fz -= pz;
+            for (int s = 0; s < smax; ++s)
+            {
+                // Lanes 0-2 ask L2 for the three component rows of slot
+                // s + kPairAhead (their 16-byte-aligned inner part, inside
+                // the atom's block), so the loads of later slots find them
+                // there.
+                if (lane < 3 && s + kPairAhead < smax)
+                {
+                    T const* r = gd + ((long)(s + kPairAhead) * 3 + lane) * cnt;
+                    unsigned long long const a =
+                        (reinterpret_cast<unsigned long long>(r + t0) + 15)
+                        & ~15ull;
+                    unsigned long long const e =
+                        reinterpret_cast<unsigned long long>(
+                            r + min(cnt, t0 + 32 * kPairChunks)) & ~15ull;
+                    if (e > a)
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;"
+                                     :: "l"(a), "r"((unsigned)(e - a))
+                                     : "memory");
+                }
+                T const* row = gd + (long)s * 3 * cnt + t0 + lane;
+#pragma unroll
+                for (int k = 0; k < kPairChunks; ++k)
+                    if (s < ns[k])
+                    {
+                        double const c = cE[eo[k] + s];
+                        T const* g = row + 32 * k;
+                        px[k] -= c * (double)g[0];
+                        py[k] -= c * (double)g[cnt];
+                        pz[k] -= c * (double)g[2 * cnt];
+                    }
+            }
+#pragma unroll
+            for (int k = 0; k < kPairChunks; ++k)
+            {
+                int const t = t0 + 32 * k + lane;
+                if (t >= cnt) continue;
+                L.pairF[(b + t) * 3 + 0] = px[k];
+                L.pairF[(b + t) * 3 + 1] = py[k];
+                L.pairF[(b + t) * 3 + 2] = pz[k];
+                fx -= px[k];
+                fy -= py[k];
+                fz -= pz[k];
+            }
         }
         fx = warpSum(fx);
         fy = warpSum(fy);

@@ -588,11 +588,17 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                 R const cr0 = invij * invij;  // 1 / r_ij^2
                 int const wb = it.pb >> 5;
                 int const we = (it.pe + 31) >> 5;
-                for (int w = wb; w < we; ++w)
+                // One loop over the lane's partners (not one per mask
+                // word): the warp's trip count is the largest partner count
+                // of its lanes, not the sum of per-word maxima.
+                int w = wb - 1;
+                unsigned m = 0u;
+                for (;;)
                 {
-                    unsigned m = NARROW ? W.bits[t * words + w] : kFull;
-                    m = rangeMask(m, w, it.pb, it.pe);
-                    while (m)
+                    while (m == 0u && ++w < we)
+                        m = rangeMask(NARROW ? W.bits[t * words + w] : kFull,
+                                      w, it.pb, it.pe);
+                    if (m == 0u) break;
                     {
                         int const k = (w << 5) + __ffs(m) - 1;
                         m &= m - 1;
@@ -784,11 +790,17 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                 R const cr0 = invij * invij;  // 1 / r_ij^2
                 int const wb = it.pb >> 5;
                 int const we = (it.pe + 31) >> 5;
-                for (int w = wb; w < we; ++w)
+                // One loop over the lane's partners (not one per mask
+                // word): the warp's trip count is the largest partner count
+                // of its lanes, not the sum of per-word maxima.
+                int w = wb - 1;
+                unsigned m = 0u;
+                for (;;)
                 {
-                    unsigned m = NARROW ? W.bits[t * words + w] : kFull;
-                    m = rangeMask(m, w, it.pb, it.pe);
-                    while (m)
+                    while (m == 0u && ++w < we)
+                        m = rangeMask(NARROW ? W.bits[t * words + w] : kFull,
+                                      w, it.pb, it.pe);
+                    if (m == 0u) break;
                     {
                         int const k = (w << 5) + __ffs(m) - 1;
                         m &= m - 1;
