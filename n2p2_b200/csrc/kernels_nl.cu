@@ -225,28 +225,60 @@ __global__ void nlCellKernel(int n, NLParams p, int numElements,
     for (int e = 0; e < kMaxElem; ++e) cntElem[e] = 0;
     int total = 0;
     long const base = (MODE == 1) ? (long)nbrOff[i] : 0;
-    for (int s = 0; s < 27; ++s)
+    // Lane s < 27 holds stencil cell s (first atom, count, image); the
+    // candidates of all 27 cells form one list of `nc` entries that the
+    // warp walks 32 at a time, so lanes stay busy across cell boundaries.
+    int cs = 0, cn = 0, bcw = 0;
+    if (lane < 27)
     {
         int bc[3];
-        int const cc = stencilCell(p, c, s, bc);
-        int const cs = cellStart[cc];
-        int const cn = cellCount[cc];
-        int const img = imgIndex(p, bc[0], bc[1], bc[2]);
-        bool const zeroShift = (bc[0] == 0 && bc[1] == 0 && bc[2] == 0);
-        for (int t0 = 0; t0 < cn; t0 += 32)
+        int const cc = stencilCell(p, c, lane, bc);
+        cs = cellStart[cc];
+        cn = cellCount[cc];
+        bcw = (bc[0] + 1) * 9 + (bc[1] + 1) * 3 + (bc[2] + 1);
+    }
+    int incl = cn;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1)
+    {
+        int const v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    int const nc = __shfl_sync(0xffffffffu, incl, 31);
+    for (int q0 = 0; q0 < nc; q0 += 32)
+    {
+        int const q = q0 + lane;
+        // Cell of candidate q: the number of cells whose inclusive count
+        // end is <= q (ends are nondecreasing over lanes).
+        int sc = 0;
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1)
         {
-            int const t = t0 + lane;
-            bool hit = false;
-            int j = 0;
-            if (t < cn)
+            int const probe = sc + step - 1;
+            int const v = __shfl_sync(0xffffffffu, incl, probe < 27 ? probe
+                                                                    : 26);
+            if (probe < 27 && v <= q) sc += step;
+        }
+        int const src = sc < 27 ? sc : 26;
+        int const endS = __shfl_sync(0xffffffffu, incl, src);
+        int const cnS = __shfl_sync(0xffffffffu, cn, src);
+        int const csS = __shfl_sync(0xffffffffu, cs, src);
+        int const bcS = __shfl_sync(0xffffffffu, bcw, src);
+        bool hit = false;
+        int j = 0;
+        int bc[3] = {bcS / 9 - 1, (bcS / 3) % 3 - 1, bcS % 3 - 1};
+        int const img = imgIndex(p, bc[0], bc[1], bc[2]);
+        if (q < nc)
+        {
+            j = cellAtoms[csS + (q - (endS - cnS))];
+            bool const zeroShift = (bc[0] == 0 && bc[1] == 0 && bc[2] == 0);
+            if (!(j == i && zeroShift))
             {
-                j = cellAtoms[cs + t];
-                if (!(j == i && zeroShift))
-                {
-                    double dr[3];
-                    hit = nlTest(p, ri, pos, j, bc[0], bc[1], bc[2], dr);
-                }
+                double dr[3];
+                hit = nlTest(p, ri, pos, j, bc[0], bc[1], bc[2], dr);
             }
+        }
+        {
             unsigned const m = __ballot_sync(0xffffffffu, hit);
             if (MODE == 0)
             {
