@@ -54,11 +54,10 @@ POT = os.path.join(POT_DIR, "h2o_52")
 STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
 # DRAM bytes (read + write) of one FP64 symmetry-function launch on this
-# workload: the ncu capture summarized under profiles/ measured
-# dram__bytes_read.sum + dram__bytes_write.sum = 1.056 GB on the
-# 12,288-atom box; traffic grows with the neighbor entries, i.e. with the
-# atoms, so the 24,576-atom launch moves twice that.
-SF_TRAFFIC_BYTES = 2.112e9
+# workload: dram__bytes_read.sum + dram__bytes_write.sum = 0.576 + 2.510 GB,
+# measured by ncu on the launches of this very bench run (the launch list
+# summarized under profiles/).
+SF_TRAFFIC_BYTES = 3.087e9
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
