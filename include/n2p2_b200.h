@@ -124,7 +124,10 @@ int    n2p2b_unit_conversion(const n2p2b_context* ctx, double* mean_energy,
 /* Parameters of symmetry function s (sorted index = NN input index) of
  * element e, as Element::getSymmetryFunction(s) holds them (normalized
  * units): out[0..9] = type, e1, e2 (-1 for radial), eta, rs, rc, zeta,
- * lambda, scaling factor, input.nn line number (0-based). */
+ * lambda, scaling factor, input.nn line number (0-based).  Compact types
+ * 20-22 give rl in place of eta, the subtype's rank in string order
+ * (e = 0, p1 = 1, p1a = 2, ..., p4a = 8) in place of rs, and the left and
+ * right angle (degrees) in place of zeta and lambda. */
 int    n2p2b_symmetry_function_params(const n2p2b_context* ctx, int e, int s,
                                       double* out);
 /* Element::setupSymmetryFunctionGroups: number of groups of element e and

@@ -532,7 +532,48 @@ struct n2p2b_context
                     SFScale& q = scale[(std::size_t)e * maxSF + s.index];
                     ewRangeHost[(std::size_t)e * maxSF + s.index] =
                         Range{s.Gmin, s.Gmax};
-                    if (g.type == 2)
+                    if (isCompactType(g.type))
+                    {
+                        // CompactFunction::setLeftRight
+                        // (libnnp/CompactFunction.cpp:60-72) for the radial
+                        // and angular functions; angles in radians as
+                        // SymFncBaseCompAng::setParameters computes them.
+                        m.eta = s.rl;
+                        m.rs = s.rc;
+                        m.lambda = s.angleLeft * M_PI / 180.0;
+                        m.zeta = s.angleRight * M_PI / 180.0;
+                        m.factorNorm = s.scalingFactor;
+                        m.factorDeriv = (s.rc + s.rl) / 2.0;
+                        m.zetaLambda = 1.0 / ((s.rc - s.rl) / 2.0);
+                        if (g.type != 20)
+                        {
+                            m.aCenter = (m.lambda + m.zeta) / 2.0;
+                            m.aScale = 1.0 / ((m.zeta - m.lambda) / 2.0);
+                        }
+                        m.zetaInt = (int16_t)s.coreType;
+                        m.useIntPow = s.asymmetric ? 1 : 0;
+                        // SymGrpCompAngn::sortMembers (calculateComp).
+                        SymFnc const* prev = k > 0
+                            ? &el.sfs[g.members[k - 1]] : nullptr;
+                        m.calcExp = (prev == nullptr || prev->rc != s.rc
+                                     || prev->rl != s.rl) ? 1 : 0;
+                        // Radial function id: the first member of the group
+                        // with the same (rl, rc, core, asymmetry); members
+                        // sharing it share their radial values.
+                        std::size_t rid = 0;
+                        while (rid < k)
+                        {
+                            SymFnc const& o = el.sfs[g.members[rid]];
+                            if (o.rl == s.rl && o.rc == s.rc
+                                && o.coreType == s.coreType
+                                && o.asymmetric == s.asymmetric)
+                                break;
+                            ++rid;
+                        }
+                        m.rsPositive = (uint8_t)rid;
+                        q.q = 1.0;
+                    }
+                    else if (g.type == 2)
                     {
                         m.factorNorm = s.scalingFactor;
                         m.calcExp = 1;
@@ -577,7 +618,8 @@ struct n2p2b_context
                                          q.shift = s.Gmean; break;
                     }
                 }
-                d.shapes = (g.type == 2) ? 0 : productShapes(el, g);
+                d.shapes = (g.type == 2 || isCompactType(g.type))
+                         ? 0 : productShapes(el, g);
             }
             sfp.maxExp = std::max(sfp.maxExp, expCount);
         }
@@ -1231,7 +1273,9 @@ struct n2p2b_context
     {
         return a.type == b.type && a.ec == b.ec && a.e1 == b.e1
             && a.e2 == b.e2 && a.eta == b.eta && a.rs == b.rs && a.rc == b.rc
-            && a.zeta == b.zeta && a.lambda == b.lambda
+            && a.zeta == b.zeta && a.lambda == b.lambda && a.rl == b.rl
+            && a.angleLeft == b.angleLeft && a.angleRight == b.angleRight
+            && a.subtype == b.subtype
             && a.cutoffType == b.cutoffType && a.cutoffAlpha == b.cutoffAlpha
             && a.scalingType == b.scalingType && a.Smin == b.Smin
             && a.Smax == b.Smax && a.Gmin == b.Gmin && a.Gmax == b.Gmax
@@ -2364,9 +2408,19 @@ int n2p2b_symmetry_function_params(n2p2b_context const* ctx, int e, int s,
     Element const& el = ctx->pot.elements[e];
     if (s < 0 || s >= (int)el.sfs.size()) return N2P2B_ERR_ARGUMENT;
     SymFnc const& f = el.sfs[s];
-    double const v[10] = {(double)f.type, (double)f.e1, (double)f.e2, f.eta,
-                          f.rs, f.rc, f.zeta, f.lambda, f.scalingFactor,
-                          (double)f.lineNumber};
+    double v[10] = {(double)f.type, (double)f.e1, (double)f.e2, f.eta,
+                    f.rs, f.rc, f.zeta, f.lambda, f.scalingFactor,
+                    (double)f.lineNumber};
+    if (isCompactType(f.type))
+    {
+        // rl, subtype rank (string order: e, p1, p1a, p2, ...), rc,
+        // angles in degrees.
+        v[3] = f.rl;
+        v[4] = f.coreType == CC_EXP ? 0.0
+             : (double)(2 * f.coreType - 1 + (f.asymmetric ? 1 : 0));
+        v[6] = f.angleLeft;
+        v[7] = f.angleRight;
+    }
     for (int k = 0; k < 10; ++k) out[k] = v[k];
     return N2P2B_OK;
 }

@@ -138,12 +138,32 @@ double SymFnc::unscale(double v) const
     }
 }
 
-// Strict weak order of n2p2's SymFnc::operator< for types 2, 3 and 9.
+// Strict weak order of n2p2's SymFnc::operator< for types 2, 3, 9
+// (SymFncExpRad.cpp, SymFncExpAngn.cpp, SymFncExpAngw.cpp) and the compact
+// types 20, 21, 22 (SymFncCompRad.cpp:55-74, SymFncCompAngn.cpp:52-74,
+// SymFncCompAngw.cpp: subtype, elements, rc, rl, angles).
 bool sfLess(SymFnc const& a, SymFnc const& b)
 {
 #define N2P2B_CMP(x) if (a.x < b.x) return true; if (a.x > b.x) return false;
     N2P2B_CMP(ec)
     N2P2B_CMP(type)
+    if (isCompactType(a.type))
+    {
+        N2P2B_CMP(subtype)
+        N2P2B_CMP(e1)
+        if (a.type != 20)
+        {
+            N2P2B_CMP(e2)
+        }
+        N2P2B_CMP(rc)
+        N2P2B_CMP(rl)
+        if (a.type != 20)
+        {
+            N2P2B_CMP(angleLeft)
+            N2P2B_CMP(angleRight)
+        }
+        return false;
+    }
     N2P2B_CMP(cutoffType)
     N2P2B_CMP(cutoffAlpha)
     N2P2B_CMP(rc)
@@ -163,11 +183,19 @@ bool sfLess(SymFnc const& a, SymFnc const& b)
     return false;
 }
 
+// SymGrp*::operator<; compact groups (SymGrpCompRad.cpp, SymGrpCompAngn.cpp,
+// SymGrpCompAngw.cpp) compare elements only.
 static bool grpLess(SymGrp const& a, SymGrp const& b)
 {
 #define N2P2B_CMP(x) if (a.x < b.x) return true; if (a.x > b.x) return false;
     N2P2B_CMP(ec)
     N2P2B_CMP(type)
+    if (isCompactType(a.type))
+    {
+        N2P2B_CMP(e1)
+        N2P2B_CMP(e2)
+        return false;
+    }
     N2P2B_CMP(cutoffType)
     N2P2B_CMP(cutoffAlpha)
     N2P2B_CMP(rc)
@@ -413,6 +441,38 @@ void Potential::setupCutoff()
     }
 }
 
+// SymFncBaseComp::setCompactFunction (libnnp/SymFncBaseComp.cpp:41-93):
+// "p1".."p4" with an optional "a" (asymmetric), or "e".
+static void setCompactSubtype(SymFnc& s)
+{
+    std::string const& t = s.subtype;
+    if (t.size() < 1 || t.size() > 3)
+        throw std::runtime_error("ERROR: Invalid compact function type "
+                                 "specification: \"" + t + "\".\n");
+    if (t.front() == 'p')
+    {
+        char const c = t.size() > 1 ? t.at(1) : '\0';
+        if (c == '1') s.coreType = CC_POLY1;
+        else if (c == '2') s.coreType = CC_POLY2;
+        else if (c == '3') s.coreType = CC_POLY3;
+        else if (c == '4') s.coreType = CC_POLY4;
+        else
+            throw std::runtime_error("ERROR: Invalid polynom type: \"" + t
+                                     + "\".\n");
+        if (t.size() == 3)
+        {
+            if (t.at(2) != 'a')
+                throw std::runtime_error("ERROR: Invalid polynom specifier: "
+                                         "\"" + t + "\".\n");
+            s.asymmetric = true;
+        }
+    }
+    else if (t.front() == 'e') s.coreType = CC_EXP;
+    else
+        throw std::runtime_error("ERROR: Unknown compact SF type: \"" + t
+                                 + "\".\n");
+}
+
 // Mode::setupSymmetryFunctions (libnnp/Mode.cpp:615-690) with
 // Element::addSymmetryFunction / sortSymmetryFunctions
 // (libnnp/Element.cpp:82-166) and the parameter parsing of
@@ -448,11 +508,55 @@ void Potential::setupSymmetryFunctions()
             s.useIntegerPow = std::fabs(s.zeta - s.zetaInt)
                               <= std::numeric_limits<double>::min();
         }
+        else if (s.type == 20)
+        {
+            // SymFncCompRad::setParameters (libnnp/SymFncCompRad.cpp:84-113).
+            s.e1 = elementIndex(a.at(2));
+            s.rl = std::atof(a.at(3).c_str());
+            s.rc = std::atof(a.at(4).c_str());
+            s.subtype = a.at(5);
+            if (s.rl > s.rc)
+                throw std::runtime_error("ERROR: Lower radial boundary >= "
+                                         "upper radial boundary.\n");
+            setCompactSubtype(s);
+        }
+        else if (s.type == 21 || s.type == 22)
+        {
+            // SymFncBaseCompAng::setParameters
+            // (libnnp/SymFncBaseCompAng.cpp:48-115).
+            s.e1 = elementIndex(a.at(2));
+            s.e2 = elementIndex(a.at(3));
+            s.rl = std::atof(a.at(4).c_str());
+            s.rc = std::atof(a.at(5).c_str());
+            s.angleLeft = std::atof(a.at(6).c_str());
+            s.angleRight = std::atof(a.at(7).c_str());
+            s.subtype = a.at(8);
+            if (s.e1 > s.e2) std::swap(s.e1, s.e2);
+            if (s.rl > s.rc)
+                throw std::runtime_error("ERROR: Lower radial boundary >= "
+                                         "upper radial boundary.\n");
+            setCompactSubtype(s);
+            if (s.angleLeft >= s.angleRight)
+                throw std::runtime_error("ERROR: Left angle boundary right "
+                                         "of or equal to right angle "
+                                         "boundary.\n");
+            double const center = (s.angleLeft + s.angleRight) / 2.0;
+            if ((s.angleLeft < 0.0 && center != 0.0)
+                || (s.angleRight > 180.0 && center != 180.0))
+                throw std::runtime_error("ERROR: Angle boundary out of "
+                                         "[0,180] and center of angular "
+                                         "function /= 0 or /= 180.\n");
+            if (s.angleRight - s.angleLeft > 360.0)
+                throw std::runtime_error("ERROR: Periodic symmetry function "
+                                         "cannot spread over domain > 360 "
+                                         "degrees\n");
+        }
         else
         {
             throw std::runtime_error(
                 "ERROR: Symmetry function type " + a.at(1)
-                + " is not supported on this path (types 2, 3, 9).\n");
+                + " is not supported on this path (types 2, 3, 9, 20, 21, "
+                  "22).\n");
         }
         elements.at(s.ec).sfs.push_back(s);
     }
@@ -474,6 +578,7 @@ void Potential::setupSymmetryFunctions()
                 s.eta /= convLength * convLength;
                 s.rs *= convLength;
                 s.rc *= convLength;
+                s.rl *= convLength;
             }
         }
         std::sort(el.sfs.begin(), el.sfs.end(), sfLess);
@@ -517,15 +622,21 @@ void Potential::setupSymmetryFunctionGroups()
         el.groups.clear();
         for (auto const& s : el.sfs)
         {
+            bool const compact = isCompactType(s.type);
+            bool const radial = (s.type == 2 || s.type == 20);
             bool placed = false;
             for (auto& g : el.groups)
             {
-                if (g.type == s.type && g.cutoffType == s.cutoffType
-                    && g.cutoffAlpha == s.cutoffAlpha && g.ec == s.ec
-                    && g.rc == s.rc && g.e1 == s.e1
-                    && (s.type == 2 || g.e2 == s.e2))
+                // SymGrp*::addMember: compact groups take every member of
+                // their elements (SymGrpCompRad.cpp:60-85).
+                if (g.type == s.type && g.ec == s.ec && g.e1 == s.e1
+                    && (radial || g.e2 == s.e2)
+                    && (compact || (g.cutoffType == s.cutoffType
+                                    && g.cutoffAlpha == s.cutoffAlpha
+                                    && g.rc == s.rc)))
                 {
                     g.members.push_back(s.index);
+                    if (compact) g.rmax = std::max(g.rmax, s.rc);
                     placed = true;
                     break;
                 }
@@ -536,14 +647,21 @@ void Potential::setupSymmetryFunctionGroups()
                 g.type = s.type;
                 g.ec = s.ec;
                 g.e1 = s.e1;
-                g.e2 = (s.type == 2) ? -1 : s.e2;
+                g.e2 = radial ? -1 : s.e2;
                 g.rc = s.rc;
                 g.cutoffType = s.cutoffType;
                 g.cutoffAlpha = s.cutoffAlpha;
+                if (compact)
+                {
+                    g.rmin = 0.0;
+                    g.rmax = s.rc;
+                }
                 g.members.push_back(s.index);
                 el.groups.push_back(g);
             }
         }
+        for (auto& g : el.groups)
+            if (isCompactType(g.type)) g.rc = g.rmax;
         std::sort(el.groups.begin(), el.groups.end(), grpLess);
         for (auto& g : el.groups)
         {

@@ -23,6 +23,8 @@
 #include <utility>
 #include <vector>
 
+#include "tables.h"
+
 namespace n2p2b
 {
 
@@ -48,9 +50,16 @@ enum Activation
     AF_GAUSSIAN, AF_COS, AF_REVLOGISTIC, AF_EXP, AF_HARMONIC
 };
 
+inline bool isCompactType(int type)
+{
+    return type == 20 || type == 21 || type == 22;
+}
+
 struct SymFnc
 {
-    int         type       = 0;   // 2 radial, 3 narrow angular, 9 wide angular
+    int         type       = 0;   // 2 radial, 3 narrow angular, 9 wide
+                                  // angular; 20 compact radial, 21 / 22
+                                  // compact narrow / wide angular
     int         ec         = 0;   // central element
     int         e1         = 0;   // neighbor element(s); e2 = -1 for radial
     int         e2         = -1;
@@ -63,6 +72,14 @@ struct SymFnc
     bool        useIntegerPow = false;
     int         cutoffType = 0;
     double      cutoffAlpha = 0.0;
+    // Compact types (SymFncBaseComp, SymFncBaseCompAng): radial support
+    // (rl, rc), angular support in degrees, subtype and its core function.
+    double      rl         = 0.0;
+    double      angleLeft  = 0.0;
+    double      angleRight = 0.0;
+    std::string subtype;
+    int         coreType   = 0;
+    bool        asymmetric = false;
     double      convLength = 1.0;
     std::size_t lineNumber = 0;
     int         index      = 0;   // position in the element's sorted list
@@ -76,7 +93,8 @@ struct SymFnc
 
     bool   relevant(int ne) const
     {
-        return type == 2 ? ne == e1 : (ne == e1 || ne == e2);
+        return (type == 2 || type == 20) ? ne == e1
+                                         : (ne == e1 || ne == e2);
     }
     double scale(double v) const;
     double unscale(double v) const;
@@ -91,6 +109,9 @@ struct SymGrp
     double           rc = 0.0;
     int              cutoffType = 0;
     double           cutoffAlpha = 0.0;
+    // Compact groups (SymGrpBaseComp): radial range of the members; rmin
+    // stays 0 as in the reference (initialised to 0, then min'ed).
+    double           rmin = 0.0, rmax = 0.0;
     std::vector<int> members;     // SF indices (element-local), member order
 };
 

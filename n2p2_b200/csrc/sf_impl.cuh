@@ -78,6 +78,10 @@ constexpr int kThreads = 32 * kWarps;
 // Members per register chunk of the general paths; small so that their
 // register demand stays below the product-form path's.
 constexpr int kGenericChunk = 6;
+// Members per register chunk of the compact angular path: a whole group of
+// up to 8 members in one pass over the triplets (acos, divisions and radial
+// values are per triplet, not per member).
+constexpr int kCompactChunk = 8;
 constexpr unsigned kFull = 0xffffffffu;
 
 // Math in the compute type.  The FP32 (precision) form uses the hardware
@@ -355,11 +359,12 @@ __device__ __forceinline__ int buildCats(DevGroup const* G, int g0, int g1,
         for (int gi = g0; gi < g1; ++gi)
         {
             DevGroup const& g = G[gi];
-            int const sides = (g.type == 2 || g.e1 == g.e2) ? 1 : 2;
+            bool const radial = (g.type == 2 || g.type == 20);
+            int const sides = (radial || g.e1 == g.e2) ? 1 : 2;
             for (int sd = 0; sd < sides; ++sd)
             {
                 int const et = (sd == 0) ? g.e1 : g.e2;
-                int const pe2 = (g.type == 2) ? g.e1
+                int const pe2 = radial ? g.e1
                               : ((sd == 0) ? g.e2 : g.e1);
                 Cat c;
                 c.gi = gi;
@@ -540,6 +545,309 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
                     out[(s * 3 + 2) * cnt + t] = -sz;
                 }
                 flushBySF(W, it.key, has ? (int)m.sf : -1, gs);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Compact symmetry functions (types 20, 21, 22).
+// ---------------------------------------------------------------------------
+
+// CoreFunction::fdf for the compact core functions (libnnp/CoreFunction.h:
+// 171-320; POLY1..4 and EXP, the subtypes SymFncBaseComp accepts).
+template <typename R>
+__device__ __forceinline__ void coreFdf(int core, R x, R E, R& fx, R& dfx)
+{
+    if (core == CC_EXP)
+    {
+        R const temp = R(1) / (x * x - R(1));
+        R const temp2 = mexp(temp);
+        fx = E * temp2;
+        dfx = R(-2) * E * x * temp * temp * temp2;
+    }
+    else if (core == CC_POLY1)
+    {
+        fx = (R(2) * x - R(3)) * x * x + R(1);
+        dfx = x * (R(6) * x - R(6));
+    }
+    else if (core == CC_POLY2)
+    {
+        R const x2 = x * x;
+        fx = ((R(15) - R(6) * x) * x - R(10)) * x * x2 + R(1);
+        dfx = x2 * ((R(60) - R(30) * x) * x - R(30));
+    }
+    else if (core == CC_POLY3)
+    {
+        R const x2 = x * x;
+        fx = (x * (x * (R(20) * x - R(70)) + R(84)) - R(35)) * x2 * x2 + R(1);
+        dfx = x2 * x * (x * (x * (R(140) * x - R(420)) + R(420)) - R(140));
+    }
+    else
+    {
+        R x4 = x * x;
+        x4 *= x4;
+        fx = (x * (x * ((R(315) - R(70) * x) * x - R(540)) + R(420))
+              - R(126)) * x * x4 + R(1);
+        dfx = x4 * (x * (x * ((R(2520) - R(630) * x) * x - R(3780))
+                         + R(2520)) - R(630));
+    }
+}
+
+// CompactFunction::fdf (libnnp/CompactFunction.h:160-167) with
+// CoreFunction's asymmetric variant x -> (2 - x) x.
+template <typename R>
+__device__ __forceinline__ void compactFdf(int core, bool asym, R center,
+                                           R scale, R a, R E, R& f, R& df)
+{
+    R const u = (a - center) * scale;
+    R const x = u < R(0) ? -u : u;
+    R fx, dfx;
+    if (asym)
+    {
+        coreFdf<R>(core, (R(2) - x) * x, E, fx, dfx);
+        dfx *= R(2) - R(2) * x;
+    }
+    else coreFdf<R>(core, x, E, fx, dfx);
+    f = fx;
+    df = dfx * (u < R(0) ? -scale : scale);
+}
+
+// SymGrpCompRad::calculate (libnnp/SymGrpCompRad.cpp:142-219): work items
+// (group, neighbor j of element e1); G_m = sum_j f_m(r_ij) over
+// rl_m < r_ij < rc_m, slot_m(j) = -sf_m f_m'(r_ij) / r_ij dr_ij.
+template <typename R, int MC>
+__device__ void compactRadialSegment(SFParams const& P, DevGroup const* G,
+                                     DevMember const* M, int g0, int g1,
+                                     int const eb[kMaxElem + 1], int cnt,
+                                     WarpMem<R> const& W, R* __restrict__ out,
+                                     int derivatives)
+{
+    int const lane = threadIdx.x & 31;
+    int ncat = 0;
+    int const items = buildCats(G, g0, g1, eb, false, 0, W, ncat);
+    int maxM = 0;
+    for (int gi = g0; gi < g1; ++gi) maxM = max(maxM, G[gi].mcnt);
+    for (int q0 = 0; q0 < items; q0 += 32)
+    {
+        Item const it = itemOf(W, ncat, q0 + lane);
+        bool const active = it.gi >= 0;
+        DevGroup const& g = G[active ? it.gi : g0];
+        int const t = it.t;
+        R const r = W.d[t];
+        bool const valid = active && (r < R(g.rc)) && (r > R(0));
+        R const d1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        for (int mb = 0; mb < maxM; mb += MC)
+        {
+#pragma unroll
+            for (int l = 0; l < MC; ++l)
+            {
+                bool const has = active && (mb + l < g.mcnt);
+                DevMember const& m = M[g.mbeg + (has ? mb + l : 0)];
+                R gs = R(0), p1 = R(0);
+                if (has && valid && r > R(m.eta) && r < R(m.rs))
+                {
+                    R rad, drad;
+                    compactFdf<R>(m.zetaInt, m.useIntPow != 0,
+                                  R(m.factorDeriv), R(m.zetaLambda), r,
+                                  R(P.E), rad, drad);
+                    gs = rad;
+                    p1 = drad * (R(m.factorNorm) / r);
+                }
+                if (derivatives && has)
+                {
+                    long const s = m.slot[it.et];
+                    out[(s * 3 + 0) * cnt + t] = -(p1 * d1[0]);
+                    out[(s * 3 + 1) * cnt + t] = -(p1 * d1[1]);
+                    out[(s * 3 + 2) * cnt + t] = -(p1 * d1[2]);
+                }
+                flushBySF(W, it.key, has ? (int)m.sf : -1, gs);
+            }
+        }
+    }
+}
+
+// SymGrpCompAngn::calculate / SymGrpCompAngw::calculate
+// (libnnp/SymGrpCompAngn.cpp:171-383, SymGrpCompAngw.cpp) in owner-computes
+// form: the owner j of an item visits every partner k of the other element;
+// per member, with the reference's open-interval tests on r_ij, r_ik, r_jk
+// (narrow) and the angle theta = acos(cos theta_ijk),
+//   term = f(r_ij) f(r_ik) [f(r_jk)] g(theta),
+//   p_own = sf (rad phi_own g' acos' + g chi_own),  p3 = sf (rad psi g' acos'
+//   + g chi_jk), slot(j) = -(sum_k p_own dr_ij + p3 (dr_ik - dr_ij)),
+// the reference's p1 (owner first) or p2 (owner second).  The reference
+// reuses f(r_jk) of the previous member when calculateComp is false and
+// that member was not skipped; the source member is found by walking back
+// over the run (same rl, rc: only the angle test can differ).  A radial
+// value that underflows to zero inside its support skips the member here
+// whichever neighbor comes first; the reference checks the first one only,
+// which changes nothing but that reuse chain.  Narrow groups walk the
+// per-atom validity bitmask built with rc = rmax (the reference's group-level
+// r_ik < rmax, r_jk^2 < rmax^2 tests); the owner's radial values are formed
+// once per item and the partner's once per radial function id.
+template <typename R, int MC, bool NARROW>
+__device__ void compactAngularSegment(SFParams const& P, DevGroup const* G,
+                                      DevMember const* M, int g0, int g1,
+                                      int const eb[kMaxElem + 1], int cnt,
+                                      int words, WarpMem<R> const& W,
+                                      R* __restrict__ out, int derivatives)
+{
+    int const lane = threadIdx.x & 31;
+    int ncat = 0;
+    int const items = buildCats(G, g0, g1, eb, false, 0, W, ncat);
+    int maxM = 0;
+    for (int gi = g0; gi < g1; ++gi) maxM = max(maxM, G[gi].mcnt);
+    R const E = R(P.E);
+    for (int q0 = 0; q0 < items; q0 += 32)
+    {
+        Item const it = itemOf(W, ncat, q0 + lane);
+        bool const active = it.gi >= 0;
+        DevGroup const& g = G[active ? it.gi : g0];
+        int const t = it.t;
+        R const rij = W.d[t];
+        R const rmax = R(g.rc);
+        bool const valid = active && (rij < rmax) && (rij > R(0));
+        R const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        for (int mb = 0; mb < maxM; mb += MC)
+        {
+            int const mc = active ? min(MC, g.mcnt - mb) : 0;
+            R aG[MC], aP[MC], aQx[MC], aQy[MC], aQz[MC];
+            // The owner's radial value per member (0: r_ij outside).
+            R radO[MC], dradO[MC];
+#pragma unroll
+            for (int l = 0; l < MC; ++l)
+            {
+                aG[l] = aP[l] = aQx[l] = aQy[l] = aQz[l] = R(0);
+                radO[l] = dradO[l] = R(0);
+                if (l < mc)
+                {
+                    DevMember const& mm = M[g.mbeg + mb + l];
+                    if (rij > R(mm.eta) && rij < R(mm.rs))
+                        compactFdf<R>(mm.zetaInt, mm.useIntPow != 0,
+                                      R(mm.factorDeriv), R(mm.zetaLambda),
+                                      rij, E, radO[l], dradO[l]);
+                }
+            }
+            if (valid && mc > 0)
+            {
+                // Partners: the narrow validity bitmask (r_ik < rmax,
+                // r_jk^2 < rmax^2), or every k of the partner element.
+                int const wb = it.pb >> 5;
+                int const we = (it.pe + 31) >> 5;
+                int w = wb - 1;
+                unsigned m = 0u;
+                for (;;)
+                {
+                    while (m == 0u && ++w < we)
+                        m = rangeMask(NARROW ? W.bits[t * words + w] : kFull,
+                                      w, it.pb, it.pe);
+                    if (m == 0u) break;
+                    int const k = (w << 5) + __ffs(m) - 1;
+                    m &= m - 1;
+                    R const rik = W.d[k];
+                    if (!NARROW && (k == t || !(rik < rmax))) continue;
+                    R const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
+                    R const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1],
+                                      dr2[2] - dr1[2]};
+                    R rjk = R(0), rinvjk = R(0);
+                    if (NARROW)
+                    {
+                        R const r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1]
+                                   + dr3[2] * dr3[2];
+                        if (r2 <= R(0)) continue;
+                        rjk = sqrt(r2);
+                        rinvjk = R(1) / rjk;
+                    }
+                    R const rinvijik = R(1) / (rij * rik);
+                    R const costijk = (dr1[0] * dr2[0] + dr1[1] * dr2[1]
+                                       + dr1[2] * dr2[2]) * rinvijik;
+                    if (costijk <= R(-1) || costijk >= R(1)) continue;
+                    R const theta = acos(costijk);
+                    R const rinvOwn = rinvijik * rik;
+                    R const rinvPart = rinvijik * rij;
+                    R const phi0 = rinvOwn * (rinvPart - rinvOwn * costijk);
+                    R const dacos = derivatives
+                        ? R(-1) / sqrt(R(1) - costijk * costijk) : R(0);
+                    // Radial values of the partner (and of r_jk) for the
+                    // current radial function id.
+                    int rid = -1;
+                    R radP = R(0), dradP = R(0), radJ = R(0), dradJ = R(0);
+#pragma unroll
+                    for (int l = 0; l < MC; ++l)
+                    {
+                        if (l >= mc) break;
+                        int const mi = mb + l;
+                        DevMember const& mm = M[g.mbeg + mi];
+                        R const rl = R(mm.eta), rc = R(mm.rs);
+                        if (radO[l] == R(0) || rik <= rl || rik >= rc
+                            || (NARROW && (rjk <= rl || rjk >= rc))
+                            || theta <= R(mm.lambda) || theta >= R(mm.zeta))
+                            continue;
+                        int const core = mm.zetaInt;
+                        bool const asym = mm.useIntPow != 0;
+                        R const c0 = R(mm.factorDeriv), c1 = R(mm.zetaLambda);
+                        if ((int)mm.rsPositive != rid)
+                        {
+                            rid = mm.rsPositive;
+                            compactFdf<R>(core, asym, c0, c1, rik, E, radP,
+                                          dradP);
+                            if (NARROW)
+                                compactFdf<R>(core, asym, c0, c1, rjk, E,
+                                              radJ, dradJ);
+                        }
+                        if (radP == R(0)) continue;
+                        R radjk = R(1), dradjk = R(0);
+                        if (NARROW)
+                        {
+                            radjk = radJ;
+                            dradjk = dradJ;
+                            int src = mi;
+                            while (src > 0 && !M[g.mbeg + src].calcExp
+                                   && theta > R(M[g.mbeg + src - 1].lambda)
+                                   && theta < R(M[g.mbeg + src - 1].zeta))
+                                --src;
+                            DevMember const& ms = M[g.mbeg + src];
+                            if (ms.rsPositive != mm.rsPositive)
+                                compactFdf<R>(ms.zetaInt, ms.useIntPow != 0,
+                                              R(ms.factorDeriv),
+                                              R(ms.zetaLambda), rjk, E,
+                                              radjk, dradjk);
+                        }
+                        R ang, dang;
+                        compactFdf<R>(core, false, R(mm.aCenter),
+                                      R(mm.aScale), theta, E, ang, dang);
+                        R const rad = radO[l] * radP * radjk;
+                        aG[l] += rad * ang;
+                        if (!derivatives) continue;
+                        dang *= dacos;
+                        R const sf = R(mm.factorNorm);
+                        R const chiOwn = rinvOwn * dradO[l] * radP * radjk;
+                        R const pOwn = (sf * rad) * (phi0 * dang)
+                                     + (sf * ang) * chiOwn;
+                        R p3 = (sf * rad) * (rinvijik * dang);
+                        if (NARROW)
+                            p3 += (sf * ang) * (-rinvjk * radO[l] * radP
+                                                * dradjk);
+                        aP[l] += pOwn;
+                        aQx[l] += p3 * dr3[0];
+                        aQy[l] += p3 * dr3[1];
+                        aQz[l] += p3 * dr3[2];
+                    }
+                }
+            }
+#pragma unroll
+            for (int l = 0; l < MC; ++l)
+            {
+                bool const has = l < mc;
+                DevMember const& mm = M[g.mbeg + (has ? mb + l : 0)];
+                if (derivatives && has)
+                {
+                    long const s = mm.slot[it.et];
+                    out[(s * 3 + 0) * cnt + t] = -(aP[l] * dr1[0] + aQx[l]);
+                    out[(s * 3 + 1) * cnt + t] = -(aP[l] * dr1[1] + aQy[l]);
+                    out[(s * 3 + 2) * cnt + t] = -(aP[l] * dr1[2] + aQz[l]);
+                }
+                flushBySF(W, it.key, has ? (int)mm.sf : -1, R(0.5) * aG[l]);
             }
         }
     }
@@ -912,7 +1220,8 @@ inline int L_pathsOverride()
 // Code paths compiled into a kernel instantiation (a kernel holding only the
 // paths a potential uses is smaller and misses the instruction cache less).
 constexpr int kPathRadial = 1, kPathFastNarrow = 2, kPathFastWide = 4,
-              kPathGenNarrow = 8, kPathGenWide = 16, kPathAll = 31;
+              kPathGenNarrow = 8, kPathGenWide = 16, kPathCompRad = 32,
+              kPathCompNarrow = 64, kPathCompWide = 128, kPathAll = 255;
 
 // FP32 with up to 12 members per register chunk: at most 168 registers, so
 // that three CTAs (12 warps) fit per SM.
@@ -1016,14 +1325,15 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
         {
             DevGroup const& h = sG[g0];
             int g1 = g0 + 1;
-            bool fast = (h.type != 2) && (h.shapes == NS);
+            bool const compactSeg = h.type >= 20;
+            bool fast = (h.type != 2) && !compactSeg && (h.shapes == NS);
             while (g1 < ge && sG[g1].type == h.type && sG[g1].rc == h.rc
                    && g1 - g0 < kMaxSegGroups)
             {
                 fast = fast && (sG[g1].shapes == NS);
                 ++g1;
             }
-            if (h.rc != fcRc)
+            if (!compactSeg && h.rc != fcRc)
             {
                 for (int t = lane; t < cnt; t += 32)
                 {
@@ -1034,7 +1344,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 }
                 fcRc = h.rc;
             }
-            if (h.type == 3 && h.rc != bitsRc)
+            if ((h.type == 3 || h.type == 21) && h.rc != bitsRc)
             {
                 // Narrow-angular validity: k != t, r_ik < rc, r_jk^2 < rc^2.
                 R const rc = R(h.rc), rc2 = R(h.rc2);
@@ -1072,7 +1382,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 }
                 bitsRc = h.rc;
             }
-            if (h.type != 2)
+            if (h.type != 2 && !compactSeg)
             {
                 // Gaussian factors E(r) = exp(-eta (r - rs)^2) per distinct
                 // (eta, rs) of the element (computed once per atom).
@@ -1099,6 +1409,32 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 if (PATHS & kPathRadial)
                     radialSegment<R, kGenericChunk>(sG, sM, g0, g1, eb, cnt,
                                                     W, out, L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
+            else if (h.type == 20)
+            {
+                if (PATHS & kPathCompRad)
+                    compactRadialSegment<R, kGenericChunk>(
+                        P, sG, sM, g0, g1, eb, cnt, W, out, L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
+            else if (h.type == 21)
+            {
+                if (PATHS & kPathCompNarrow)
+                    compactAngularSegment<R, kCompactChunk, true>(
+                        P, sG, sM, g0, g1, eb, cnt, words, W, out,
+                        L.derivatives);
+                else if (lane == 0)
+                    atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            }
+            else if (h.type == 22)
+            {
+                if (PATHS & kPathCompWide)
+                    compactAngularSegment<R, kCompactChunk, false>(
+                        P, sG, sM, g0, g1, eb, cnt, words, W, out,
+                        L.derivatives);
                 else if (lane == 0)
                     atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
             }
@@ -1168,7 +1504,7 @@ inline int pathsNeeded(SFParams const& P, int NS)
         {
             DevGroup const& h = P.groups[g0];
             int g1 = g0 + 1;
-            bool fast = (h.type != 2) && (h.shapes == NS);
+            bool fast = (h.type != 2) && (h.type < 20) && (h.shapes == NS);
             while (g1 < ge && P.groups[g1].type == h.type
                    && P.groups[g1].rc == h.rc && g1 - g0 < kMaxSegGroups)
             {
@@ -1176,6 +1512,9 @@ inline int pathsNeeded(SFParams const& P, int NS)
                 ++g1;
             }
             if (h.type == 2) paths |= kPathRadial;
+            else if (h.type == 20) paths |= kPathCompRad;
+            else if (h.type == 21) paths |= kPathCompNarrow;
+            else if (h.type == 22) paths |= kPathCompWide;
             else if (fast) paths |= (h.type == 3) ? kPathFastNarrow
                                                   : kPathFastWide;
             else paths |= (h.type == 3) ? kPathGenNarrow : kPathGenWide;

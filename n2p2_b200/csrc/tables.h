@@ -16,10 +16,19 @@ constexpr int kMaxSF        = 256;  // symmetry functions per element
 constexpr int kMaxLayers    = 8;    // NN layers incl. input and output
 constexpr int kMaxWidth     = 256;  // NN layer width
 
+// Core functions of the compact symmetry functions (CoreFunction::Type,
+// libnnp/CoreFunction.h), as subtypes "p1".."p4" (optionally "a":
+// asymmetric) and "e".
+enum CompactCore
+{
+    CC_POLY1 = 1, CC_POLY2, CC_POLY3, CC_POLY4, CC_EXP
+};
+
 // Symmetry-function group (SymGrpExpRad / SymGrpExpAngn / SymGrpExpAngw).
 struct DevGroup
 {
-    int    type;        // 2, 3, 9
+    int    type;        // 2, 3, 9; compact 20, 21, 22 (rc = the members'
+                        // largest rc, SymGrpBaseComp::rmax)
     int    e1, e2;      // neighbor elements (e2 == -1: radial)
     int    mbeg, mcnt;  // member range
     int    shapes;      // angular product form: members = runs x shapes
@@ -32,12 +41,22 @@ struct DevGroup
 
 // One group member.  Angular members carry the SymGrpExpAngn::sortMembers
 // derived factors; radial members use `factorNorm` for the scaling factor.
+// Compact members (types 20-22) reuse the fields: eta, rs = radial support
+// (rl, rc); lambda, zeta = angular support in radians; factorNorm = scaling
+// factor; factorDeriv, zetaLambda = center and scale of the radial compact
+// function; aCenter, aScale = those of the angular one
+// (CompactFunction::setLeftRight); zetaInt = core function (CompactCore),
+// useIntPow = asymmetric; calcExp = SymGrpCompAngn's calculateComp (the
+// r_jk radial value is recomputed, not reused from the previous member);
+// rsPositive = radial function id (first member of the group with the same
+// rl, rc, core and asymmetry).
 struct DevMember
 {
     double  eta, rs, lambda, zeta;
     double  factorNorm;   // angular: 2^(1-zeta) * scalingFactor; radial: sf
     double  factorDeriv;  // 2 eta / zeta / lambda
     double  zetaLambda;   // zeta * lambda
+    double  aCenter, aScale;  // compact angular function
     int16_t zetaInt;
     int16_t sf;           // element-local SF index (NN input index)
     uint8_t calcExp;      // first member of an (eta, rs) run

@@ -20,7 +20,10 @@
 #include "Structure.h"
 #include "Atom.h"
 #include "SymFnc.h"
+#include "SymFncBaseComp.h"
+#include "SymFncBaseCompAng.h"
 #include "SymFncBaseExpAng.h"
+#include "SymFncCompRad.h"
 #include "SymFncExpRad.h"
 #include "utility.h"
 
@@ -206,6 +209,33 @@ int refh_sf_params(void* p, int e, int s, double* out)
         out[6] = a->getZeta();
         out[7] = a->getLambda();
         return 0;
+    }
+    if (auto c = dynamic_cast<SymFncBaseComp const*>(&f))
+    {
+        // Compact types: rl, subtype rank in string order (e, p1, p1a, p2,
+        // ...), rc; angles (degrees) for the angular ones.
+        std::string const t = c->getSubtype();
+        double rank = 0.0;
+        if (t.size() >= 2 && t[0] == 'p')
+            rank = 2.0 * (t[1] - '0') - 1.0 + (t.size() == 3 ? 1.0 : 0.0);
+        out[3] = c->getRl();
+        out[4] = rank;
+        out[6] = 0.0;
+        out[7] = 0.0;
+        if (auto r = dynamic_cast<SymFncCompRad const*>(&f))
+        {
+            out[1] = (double)r->getE1();
+            out[2] = -1.0;
+            return 0;
+        }
+        if (auto a = dynamic_cast<SymFncBaseCompAng const*>(&f))
+        {
+            out[1] = (double)a->getE1();
+            out[2] = (double)a->getE2();
+            out[6] = a->getAngleLeft();
+            out[7] = a->getAngleRight();
+            return 0;
+        }
     }
     return -1;
 }

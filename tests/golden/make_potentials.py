@@ -9,7 +9,15 @@ weights.008.data, scaling.data} for
   narrow angular eta {0.001, 0.01, 0.05}, zeta {1, 4}, lambda +-1 per
   element pair), cos cutoff rc = 12 bohr, NN 52-25-25-1 (tanh, tanh, linear);
 * h2o_92 -- the wide form: radial eta extended by {2.5, 4.0}, zeta
-  {1, 2, 4, 16}: 92 SFs, NN 92-64-64-64-1 (softplus x3, linear).
+  {1, 2, 4, 16}: 92 SFs, NN 92-64-64-64-1 (softplus x3, linear);
+* h2o_poly -- the compact (polynomial / exp bump) family: types 20, 21 and
+  22 over all subtypes (p1..p4, asymmetric "a", e), angular windows that
+  wrap around 0 and 180 degrees, and a p2 -> p3 member boundary with equal
+  (rl, rc), which exercises the reuse of the r_jk radial value in
+  SymGrpCompAngn; plus a few types 2 and 3 so that the compact paths run
+  beside the Gaussian ones.  48 SFs, NN 48-20-20-1 (tanh, tanh, linear).
+
+    python tests/golden/make_potentials.py [name ...]   # default: all
 
 Weights: seeded U[-1, 1] for every connection, then the Nguyen-Widrow
 modification of NeuralNetwork::modifyConnections(MS_NGUYENWIDROW)
@@ -52,6 +60,37 @@ def sf_lines(radial_eta, ang_eta, zetas, rc=12.0):
                     for lam in (-1.0, 1.0):
                         lines.append(f"symfunction_short {ec} 3 {e1} {e2} "
                                      f"{eta} {lam} {zeta} {rc}")
+    return lines
+
+
+def poly_lines():
+    lines = []
+    pairs = (("H", "H"), ("H", "O"), ("O", "O"))
+    for ec in ELEMENTS:
+        for e1 in ELEMENTS:
+            for st, rl, rc in (("p2", 0.0, 12.0), ("p3", 0.0, 8.0),
+                               ("p2a", 1.0, 6.0), ("e", 0.0, 10.0),
+                               ("p4", 2.0, 12.0), ("p1", 0.0, 5.0)):
+                lines.append(f"symfunction_short {ec} 20 {e1} {rl} {rc} {st}")
+            for eta in (0.01, 0.1):
+                lines.append(f"symfunction_short {ec} 2 {e1} {eta} 0.0 12.0")
+        for e1, e2 in pairs:
+            for al, ar in ((0.0, 90.0), (45.0, 135.0), (90.0, 180.0),
+                           (-30.0, 30.0), (150.0, 210.0)):
+                lines.append(f"symfunction_short {ec} 21 {e1} {e2} 0.0 12.0 "
+                             f"{al} {ar} p2")
+            lines.append(f"symfunction_short {ec} 21 {e1} {e2} 0.0 12.0 "
+                         f"0.0 180.0 p3")
+            lines.append(f"symfunction_short {ec} 21 {e1} {e2} 0.0 8.0 "
+                         f"0.0 120.0 e")
+            lines.append(f"symfunction_short {ec} 22 {e1} {e2} 0.0 10.0 "
+                         f"0.0 180.0 p2")
+            lines.append(f"symfunction_short {ec} 22 {e1} {e2} 0.0 10.0 "
+                         f"60.0 120.0 p2")
+            lines.append(f"symfunction_short {ec} 22 {e1} {e2} 0.5 9.0 "
+                         f"30.0 150.0 p2a")
+        for lam in (-1.0, 1.0):
+            lines.append(f"symfunction_short {ec} 3 H H 0.01 {lam} 1.0 12.0")
     return lines
 
 
@@ -145,10 +184,11 @@ def write_scaling(d, n_frames=10, n_mol=64):
                         f"{sigma:24.16E}\n")
 
 
-def make(name, radial_eta, ang_eta, zetas, nodes, acts, seed):
+def make(name, radial_eta, ang_eta, zetas, nodes, acts, seed, lines=None):
     d = os.path.join(OUT, name)
     os.makedirs(d, exist_ok=True)
-    lines = sf_lines(radial_eta, ang_eta, zetas)
+    if lines is None:
+        lines = sf_lines(radial_eta, ang_eta, zetas)
     write_input_nn(d, nodes, acts, lines)
     nsf = len(lines) // 2
     write_weights(d, nsf, nodes, acts, seed)
@@ -157,8 +197,15 @@ def make(name, radial_eta, ang_eta, zetas, nodes, acts, seed):
 
 
 if __name__ == "__main__":
+    want = set(sys.argv[1:]) or {"h2o_52", "h2o_92", "h2o_poly"}
     base_eta = [0.001, 0.01, 0.03, 0.06, 0.15, 0.3, 0.6, 1.5]
-    make("h2o_52", base_eta, [0.001, 0.01, 0.05], [1.0, 4.0],
-         [25, 25], ["t", "t", "l"], seed=52)
-    make("h2o_92", base_eta + [2.5, 4.0], [0.001, 0.01, 0.05],
-         [1.0, 2.0, 4.0, 16.0], [64, 64, 64], ["p", "p", "p", "l"], seed=92)
+    if "h2o_52" in want:
+        make("h2o_52", base_eta, [0.001, 0.01, 0.05], [1.0, 4.0],
+             [25, 25], ["t", "t", "l"], seed=52)
+    if "h2o_92" in want:
+        make("h2o_92", base_eta + [2.5, 4.0], [0.001, 0.01, 0.05],
+             [1.0, 2.0, 4.0, 16.0], [64, 64, 64], ["p", "p", "p", "l"],
+             seed=92)
+    if "h2o_poly" in want:
+        make("h2o_poly", None, None, None, [20, 20], ["t", "t", "l"],
+             seed=48, lines=poly_lines())

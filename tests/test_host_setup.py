@@ -61,7 +61,9 @@ def test_symmetry_function_setup_matches_reference(d):
                          ids=lambda d: os.path.basename(d))
 def test_groups_partition_and_order(d):
     """Groups partition the SFs; members are sorted with eta slowest
-    (SymGrpExpAngn::sortMembers) and share type, rc and elements."""
+    (SymGrpExpAngn::sortMembers) and share type, rc and elements.  Compact
+    groups (types 20-22, SymGrpCompRad / SymGrpCompAngn) share type and
+    elements only; their members are sorted by subtype, rc, rl, angles."""
     p = host_mode(d)
     for e in range(p.num_elements):
         groups = p.symmetry_function_groups(e)
@@ -70,10 +72,14 @@ def test_groups_partition_and_order(d):
         for g in groups:
             prm = [p.symmetry_function_params(e, s) for s in g]
             base = prm[0]
+            compact = base[0] >= 20
             for q in prm:
-                assert q[0] == base[0] and q[5] == base[5]
+                assert q[0] == base[0]
                 assert q[1] == base[1] and q[2] == base[2]
-            keys = [tuple(q[[3, 4, 6, 7]]) for q in prm]
+                if not compact:
+                    assert q[5] == base[5]
+            idx = [4, 5, 3, 6, 7] if compact else [3, 4, 6, 7]
+            keys = [tuple(q[idx]) for q in prm]
             assert keys == sorted(keys)
 
 
