@@ -15,7 +15,10 @@ weights.008.data, scaling.data} for
   wrap around 0 and 180 degrees, and a p2 -> p3 member boundary with equal
   (rl, rc), which exercises the reuse of the r_jk radial value in
   SymGrpCompAngn; plus a few types 2 and 3 so that the compact paths run
-  beside the Gaussian ones.  48 SFs, NN 48-20-20-1 (tanh, tanh, linear).
+  beside the Gaussian ones.  48 SFs, NN 48-20-20-1 (tanh, tanh, linear);
+* h2o_wtd -- the element-weighted Gaussian family: types 12 and 13
+  (weights: atomic numbers), with rs = 0 and rs > 0 members, beside a few
+  types 2 and 3.  21 SFs, NN 21-15-15-1 (tanh, tanh, linear).
 
     python tests/golden/make_potentials.py [name ...]   # default: all
 
@@ -89,6 +92,26 @@ def poly_lines():
                          f"60.0 120.0 p2")
             lines.append(f"symfunction_short {ec} 22 {e1} {e2} 0.5 9.0 "
                          f"30.0 150.0 p2a")
+        for lam in (-1.0, 1.0):
+            lines.append(f"symfunction_short {ec} 3 H H 0.01 {lam} 1.0 12.0")
+    return lines
+
+
+def wtd_lines():
+    lines = []
+    for ec in ELEMENTS:
+        for eta, rs in ((0.001, 0.0), (0.01, 0.0), (0.03, 0.0), (0.1, 0.0),
+                        (0.3, 0.0), (0.5, 2.0)):
+            lines.append(f"symfunction_short {ec} 12 {eta} {rs} 12.0")
+        for eta in (0.001, 0.01):
+            for zeta in (1.0, 4.0):
+                for lam in (-1.0, 1.0):
+                    lines.append(f"symfunction_short {ec} 13 {eta} 0.0 "
+                                 f"{lam} {zeta} 12.0")
+        lines.append(f"symfunction_short {ec} 13 0.02 1.0 1.0 2.0 12.0")
+        for e1 in ELEMENTS:
+            for eta in (0.01, 0.1):
+                lines.append(f"symfunction_short {ec} 2 {e1} {eta} 0.0 12.0")
         for lam in (-1.0, 1.0):
             lines.append(f"symfunction_short {ec} 3 H H 0.01 {lam} 1.0 12.0")
     return lines
@@ -197,7 +220,7 @@ def make(name, radial_eta, ang_eta, zetas, nodes, acts, seed, lines=None):
 
 
 if __name__ == "__main__":
-    want = set(sys.argv[1:]) or {"h2o_52", "h2o_92", "h2o_poly"}
+    want = set(sys.argv[1:]) or {"h2o_52", "h2o_92", "h2o_poly", "h2o_wtd"}
     base_eta = [0.001, 0.01, 0.03, 0.06, 0.15, 0.3, 0.6, 1.5]
     if "h2o_52" in want:
         make("h2o_52", base_eta, [0.001, 0.01, 0.05], [1.0, 4.0],
@@ -209,3 +232,6 @@ if __name__ == "__main__":
     if "h2o_poly" in want:
         make("h2o_poly", None, None, None, [20, 20], ["t", "t", "l"],
              seed=48, lines=poly_lines())
+    if "h2o_wtd" in want:
+        make("h2o_wtd", None, None, None, [15, 15], ["t", "t", "l"],
+             seed=21, lines=wtd_lines())

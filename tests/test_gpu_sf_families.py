@@ -1,12 +1,16 @@
-"""GPU parity of the compact symmetry functions (types 20, 21, 22:
-SymGrpCompRad, SymGrpCompAngn, SymGrpCompAngw) against the reference library.
+"""GPU parity of the symmetry-function families beyond types 2, 3 and 9
+against the reference library.
 
-The potential `tests/golden/potentials/h2o_poly` (written by
-tests/golden/make_potentials.py, scaling statistics from the reference
-itself) uses every compact subtype (p1..p4, asymmetric p2a, e), angular
-windows that wrap around 0 and 180 degrees, a p2 -> p3 member boundary with
-equal (rl, rc) -- where the reference reuses the previous member's r_jk
-radial value -- and a few Gaussian types 2 and 3 beside them.
+* `h2o_poly`: the compact functions (types 20, 21, 22: SymGrpCompRad,
+  SymGrpCompAngn, SymGrpCompAngw) with every subtype (p1..p4, asymmetric
+  p2a, e), angular windows that wrap around 0 and 180 degrees, a p2 -> p3
+  member boundary with equal (rl, rc) -- where the reference reuses the
+  previous member's r_jk radial value -- and a few types 2 and 3 beside them;
+* `h2o_wtd`: the element-weighted Gaussian functions (types 12, 13:
+  SymGrpExpRadWeighted, SymGrpExpAngnWeighted) with rs = 0 and rs > 0.
+
+Both potentials are written by tests/golden/make_potentials.py with
+scaling statistics from the reference itself.
 
 Tolerances as in test_gpu_parity.py: symmetry functions, dE/dG and dG/dr
 1e-12 of the array's scale; energy 1e-10 relative; forces
@@ -22,8 +26,8 @@ from n2p2_b200 import synth
 
 pytestmark = pytest.mark.gpu
 
-POT = os.path.join(os.path.dirname(__file__), "golden", "potentials",
-                   "h2o_poly")
+POTS = os.path.join(os.path.dirname(__file__), "golden", "potentials")
+FAMILIES = ["h2o_poly", "h2o_wtd"]
 
 
 @pytest.fixture(scope="module")
@@ -34,18 +38,20 @@ def gpu():
     return torch
 
 
-def _models(precision="fp64"):
+def _models(name, precision="fp64"):
     from n2p2_b200.mode import Prediction
     from oracle.ref import RefModel
-    p = Prediction(POT)
+    d = os.path.join(POTS, name)
+    p = Prediction(d)
     p.setup()
     p.set_precision(precision)
-    return p, RefModel(POT)
+    return p, RefModel(d)
 
 
+@pytest.mark.parametrize("name", FAMILIES)
 @pytest.mark.parametrize("nmol,seed", [(64, 3), (128, 8)])
-def test_compact_intermediates_match(gpu, nmol, seed):
-    p, ref = _models()
+def test_family_intermediates_match(gpu, name, nmol, seed):
+    p, ref = _models(name)
     box, pos, elem = synth.water_box(nmol, seed)
     ref.set_structure(pos, elem, box)
     ref.evaluate(True)
@@ -64,9 +70,10 @@ def test_compact_intermediates_match(gpu, nmol, seed):
     assert np.abs(n0 - n1).max() <= 1e-12 * np.abs(n0).max()
 
 
+@pytest.mark.parametrize("name", FAMILIES)
 @pytest.mark.parametrize("nmol,seed", [(64, 5), (512, 9)])
-def test_compact_energy_forces(gpu, nmol, seed):
-    p, ref = _models()
+def test_family_energy_forces(gpu, name, nmol, seed):
+    p, ref = _models(name)
     box, pos, elem = synth.water_box(nmol, seed)
     ref.set_structure(pos, elem, box)
     e0, f0 = ref.predict()
@@ -76,8 +83,9 @@ def test_compact_energy_forces(gpu, nmol, seed):
     assert np.all(np.abs(f1 - f0) <= 1e-10 * scale)
 
 
-def test_compact_mixed_form_accuracy(gpu):
-    p, ref = _models("mixed")
+@pytest.mark.parametrize("name", FAMILIES)
+def test_family_mixed_form_accuracy(gpu, name):
+    p, ref = _models(name, "mixed")
     box, pos, elem = synth.water_box(256, 13)
     n = len(pos)
     rng = np.random.default_rng(13)
