@@ -468,6 +468,8 @@ struct n2p2b_context
         sfp.cutoffType = pot.cutoffType;
         sfp.maxSlots = maxSlots;
         sfp.maxSF = maxSF;
+        for (int e = 0; e < ne && e < kMaxElem; ++e)
+            sfp.atomicNumber[e] = pot.elements[e].atomicNumber;
         sfp.PI = 4.0 * std::atan(1.0);
         sfp.PI_2 = 2.0 * std::atan(1.0);
         sfp.E = std::exp(1.0);
@@ -545,7 +547,7 @@ struct n2p2b_context
                         m.factorNorm = s.scalingFactor;
                         m.factorDeriv = (s.rc + s.rl) / 2.0;
                         m.zetaLambda = 1.0 / ((s.rc - s.rl) / 2.0);
-                        if (g.type != 20)
+                        if (g.type != 20 && g.type != 23)
                         {
                             m.aCenter = (m.lambda + m.zeta) / 2.0;
                             m.aScale = 1.0 / ((m.zeta - m.lambda) / 2.0);
@@ -573,7 +575,7 @@ struct n2p2b_context
                         m.rsPositive = (uint8_t)rid;
                         q.q = 1.0;
                     }
-                    else if (g.type == 2)
+                    else if (g.type == 2 || g.type == 12)
                     {
                         m.factorNorm = s.scalingFactor;
                         m.calcExp = 1;
@@ -618,7 +620,8 @@ struct n2p2b_context
                                          q.shift = s.Gmean; break;
                     }
                 }
-                d.shapes = (g.type == 2 || isCompactType(g.type))
+                d.shapes = (g.type == 2 || g.type == 12 || g.type == 13
+                            || isCompactType(g.type))
                          ? 0 : productShapes(el, g);
             }
             sfp.maxExp = std::max(sfp.maxExp, expCount);

@@ -151,13 +151,13 @@ bool sfLess(SymFnc const& a, SymFnc const& b)
     {
         N2P2B_CMP(subtype)
         N2P2B_CMP(e1)
-        if (a.type != 20)
+        if (a.type != 20 && a.type != 23)
         {
             N2P2B_CMP(e2)
         }
         N2P2B_CMP(rc)
         N2P2B_CMP(rl)
-        if (a.type != 20)
+        if (a.type != 20 && a.type != 23)
         {
             N2P2B_CMP(angleLeft)
             N2P2B_CMP(angleRight)
@@ -508,6 +508,30 @@ void Potential::setupSymmetryFunctions()
             s.useIntegerPow = std::fabs(s.zeta - s.zetaInt)
                               <= std::numeric_limits<double>::min();
         }
+        else if (s.type == 12)
+        {
+            // SymFncExpRadWeighted::setParameters
+            // (libnnp/SymFncExpRadWeighted.cpp:76-90): no element.
+            s.e1 = -1;
+            s.eta = std::atof(a.at(2).c_str());
+            s.rs = std::atof(a.at(3).c_str());
+            s.rc = std::atof(a.at(4).c_str());
+        }
+        else if (s.type == 13)
+        {
+            // SymFncExpAngnWeighted::setParameters
+            // (libnnp/SymFncExpAngnWeighted.cpp:89-115).
+            s.e1 = -1;
+            s.e2 = -1;
+            s.eta = std::atof(a.at(2).c_str());
+            s.rs = std::atof(a.at(3).c_str());
+            s.lambda = std::atof(a.at(4).c_str());
+            s.zeta = std::atof(a.at(5).c_str());
+            s.rc = std::atof(a.at(6).c_str());
+            s.zetaInt = (int)std::round(s.zeta);
+            s.useIntegerPow = std::fabs(s.zeta - s.zetaInt)
+                              <= std::numeric_limits<double>::min();
+        }
         else if (s.type == 20)
         {
             // SymFncCompRad::setParameters (libnnp/SymFncCompRad.cpp:84-113).
@@ -520,17 +544,33 @@ void Potential::setupSymmetryFunctions()
                                          "upper radial boundary.\n");
             setCompactSubtype(s);
         }
-        else if (s.type == 21 || s.type == 22)
+        else if (s.type == 23)
+        {
+            // SymFncCompRadWeighted::setParameters
+            // (libnnp/SymFncCompRadWeighted.cpp:68-94): no element.
+            s.e1 = -1;
+            s.rl = std::atof(a.at(2).c_str());
+            s.rc = std::atof(a.at(3).c_str());
+            s.subtype = a.at(4);
+            if (s.rl > s.rc)
+                throw std::runtime_error("ERROR: Lower radial boundary >= "
+                                         "upper radial boundary.\n");
+            setCompactSubtype(s);
+        }
+        else if (s.type >= 21 && s.type <= 25)
         {
             // SymFncBaseCompAng::setParameters
-            // (libnnp/SymFncBaseCompAng.cpp:48-115).
-            s.e1 = elementIndex(a.at(2));
-            s.e2 = elementIndex(a.at(3));
-            s.rl = std::atof(a.at(4).c_str());
-            s.rc = std::atof(a.at(5).c_str());
-            s.angleLeft = std::atof(a.at(6).c_str());
-            s.angleRight = std::atof(a.at(7).c_str());
-            s.subtype = a.at(8);
+            // (libnnp/SymFncBaseCompAng.cpp:48-115); the weighted forms
+            // (SymFncBaseCompAngWeighted.cpp:46-100) have no elements.
+            bool const w = (s.type == 24 || s.type == 25);
+            int const o = w ? 0 : 2;
+            s.e1 = w ? -1 : elementIndex(a.at(2));
+            s.e2 = w ? -1 : elementIndex(a.at(3));
+            s.rl = std::atof(a.at(2 + o).c_str());
+            s.rc = std::atof(a.at(3 + o).c_str());
+            s.angleLeft = std::atof(a.at(4 + o).c_str());
+            s.angleRight = std::atof(a.at(5 + o).c_str());
+            s.subtype = a.at(6 + o);
             if (s.e1 > s.e2) std::swap(s.e1, s.e2);
             if (s.rl > s.rc)
                 throw std::runtime_error("ERROR: Lower radial boundary >= "
@@ -555,8 +595,8 @@ void Potential::setupSymmetryFunctions()
         {
             throw std::runtime_error(
                 "ERROR: Symmetry function type " + a.at(1)
-                + " is not supported on this path (types 2, 3, 9, 20, 21, "
-                  "22).\n");
+                + " is not supported on this path (types 2, 3, 9, 12, 13, "
+                  "20-25).\n");
         }
         elements.at(s.ec).sfs.push_back(s);
     }
@@ -623,7 +663,8 @@ void Potential::setupSymmetryFunctionGroups()
         for (auto const& s : el.sfs)
         {
             bool const compact = isCompactType(s.type);
-            bool const radial = (s.type == 2 || s.type == 20);
+            bool const radial = (s.type == 2 || s.type == 12
+                                 || s.type == 20 || s.type == 23);
             bool placed = false;
             for (auto& g : el.groups)
             {

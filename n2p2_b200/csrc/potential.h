@@ -52,14 +52,26 @@ enum Activation
 
 inline bool isCompactType(int type)
 {
-    return type == 20 || type == 21 || type == 22;
+    return type >= 20 && type <= 25;
+}
+
+// Element-weighted types (SymFncExpRadWeighted, SymFncExpAngnWeighted,
+// SymFncCompRadWeighted, SymFncCompAngnWeighted, SymFncCompAngwWeighted):
+// every neighbor element counts, weighted by its atomic number.
+inline bool isWeightedType(int type)
+{
+    return type == 12 || type == 13 || type == 23 || type == 24
+        || type == 25;
 }
 
 struct SymFnc
 {
     int         type       = 0;   // 2 radial, 3 narrow angular, 9 wide
-                                  // angular; 20 compact radial, 21 / 22
-                                  // compact narrow / wide angular
+                                  // angular; 12 / 13 element-weighted
+                                  // radial / narrow angular; 20 compact
+                                  // radial, 21 / 22 compact narrow / wide
+                                  // angular; 23 / 24 / 25 their
+                                  // element-weighted forms
     int         ec         = 0;   // central element
     int         e1         = 0;   // neighbor element(s); e2 = -1 for radial
     int         e2         = -1;
@@ -93,6 +105,7 @@ struct SymFnc
 
     bool   relevant(int ne) const
     {
+        if (isWeightedType(type)) return true;
         return (type == 2 || type == 20) ? ne == e1
                                          : (ne == e1 || ne == e2);
     }

@@ -278,6 +278,13 @@ struct Cat
 // are split), so the category table never overflows.
 constexpr int kMaxSegGroups = 16;
 constexpr int kMaxCats = 2 * kMaxSegGroups;
+// Groups per segment: element-weighted groups give one category per owner
+// element, the others at most two.
+__host__ __device__ constexpr int segCap(int type)
+{
+    return (type == 12 || type == 13 || type >= 23) ? kMaxCats / kMaxElem
+                                                    : kMaxSegGroups;
+}
 constexpr long kCatsBytes = ((long)(kMaxCats * sizeof(Cat)) + 15) / 16 * 16;
 
 // The balanced owner order and its sort scratch (see WarpMem).
@@ -359,6 +366,26 @@ __device__ __forceinline__ int buildCats(DevGroup const* G, int g0, int g1,
         for (int gi = g0; gi < g1; ++gi)
         {
             DevGroup const& g = G[gi];
+            if (g.type == 12 || g.type == 13 || g.type >= 23)
+            {
+                // Element-weighted groups: owners of every element,
+                // partners of every element.
+                for (int et = 0; et < kMaxElem; ++et)
+                {
+                    if (eb[et + 1] <= eb[et]) continue;
+                    Cat c;
+                    c.gi = gi;
+                    c.et = et;
+                    c.ob = eb[et];
+                    c.on = eb[et + 1] - eb[et];
+                    c.pb = 0;
+                    c.pe = eb[kMaxElem];
+                    c.oo = -1;
+                    W.cats[n++] = c;
+                    total += c.on;
+                }
+                continue;
+            }
             bool const radial = (g.type == 2 || g.type == 20);
             int const sides = (radial || g.e1 == g.e2) ? 1 : 2;
             for (int sd = 0; sd < sides; ++sd)
@@ -497,8 +524,9 @@ __device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
 }
 
 template <typename R, int MC>
-__device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
-                              int g1, int const eb[kMaxElem + 1], int cnt,
+__device__ void radialSegment(SFParams const& P, DevGroup const* G,
+                              DevMember const* M, int g0, int g1,
+                              int const eb[kMaxElem + 1], int cnt,
                               WarpMem<R> const& W, R* __restrict__ out,
                               int derivatives)
 {
@@ -517,6 +545,8 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
         bool const valid = active && (r < R(g.rc));
         R const pfc = W.fc[t], pdfcr = W.dfcr[t], inv = W.inv[t];
         R const d1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        // SymGrpExpRadWeighted (type 12): weight = atomic number of j.
+        R const z = (g.type == 12) ? R(P.atomicNumber[it.et]) : R(1);
         for (int mb = 0; mb < maxM; mb += MC)
         {
 #pragma unroll
@@ -531,7 +561,7 @@ __device__ void radialSegment(DevGroup const* G, DevMember const* M, int g0,
                     // written as f_c'/r - 2 eta (r - rs) f_c / r.
                     R const eta = R(m.eta);
                     R const rr = r - R(m.rs);
-                    R const pexp = mexp(-eta * rr * rr);
+                    R const pexp = z * mexp(-eta * rr * rr);
                     gs = pexp * pfc;
                     p1 = R(m.factorNorm)
                        * (pdfcr - R(2) * eta * rr * pfc * inv) * pexp;
@@ -637,6 +667,8 @@ __device__ void compactRadialSegment(SFParams const& P, DevGroup const* G,
         R const r = W.d[t];
         bool const valid = active && (r < R(g.rc)) && (r > R(0));
         R const d1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+        // SymGrpCompRadWeighted (type 23): weight = atomic number of j.
+        R const z = (g.type == 23) ? R(P.atomicNumber[it.et]) : R(1);
         for (int mb = 0; mb < maxM; mb += MC)
         {
 #pragma unroll
@@ -651,8 +683,8 @@ __device__ void compactRadialSegment(SFParams const& P, DevGroup const* G,
                     compactFdf<R>(m.zetaInt, m.useIntPow != 0,
                                   R(m.factorDeriv), R(m.zetaLambda), r,
                                   R(P.E), rad, drad);
-                    gs = rad;
-                    p1 = drad * (R(m.factorNorm) / r);
+                    gs = z * rad;
+                    p1 = drad * (z * R(m.factorNorm) / r);
                 }
                 if (derivatives && has)
                 {
@@ -768,6 +800,15 @@ __device__ void compactAngularSegment(SFParams const& P, DevGroup const* G,
                     R const phi0 = rinvOwn * (rinvPart - rinvOwn * costijk);
                     R const dacos = derivatives
                         ? R(-1) / sqrt(R(1) - costijk * costijk) : R(0);
+                    // SymGrpCompAng[nw]Weighted (types 24, 25): weight
+                    // Z_j Z_k on the term and its derivatives.
+                    R zz = R(1);
+                    if (g.type >= 24)
+                    {
+                        int ek = 0;
+                        while (k >= eb[ek + 1]) ++ek;
+                        zz = R(P.atomicNumber[it.et] * P.atomicNumber[ek]);
+                    }
                     // Radial values of the partner (and of r_jk) for the
                     // current radial function id.
                     int rid = -1;
@@ -816,6 +857,8 @@ __device__ void compactAngularSegment(SFParams const& P, DevGroup const* G,
                         R ang, dang;
                         compactFdf<R>(core, false, R(mm.aCenter),
                                       R(mm.aScale), theta, E, ang, dang);
+                        ang *= zz;
+                        dang *= zz;
                         R const rad = radO[l] * radP * radjk;
                         aG[l] += rad * ang;
                         if (!derivatives) continue;
@@ -947,6 +990,17 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
                         {
                             pfc = pfcij * pfcik;
                             pr1 = pfcik * pdfcrij;
+                        }
+                        if (NARROW && g.type == 13)
+                        {
+                            // SymGrpExpAngnWeighted: weight Z_j Z_k.
+                            int ek = 0;
+                            while (k >= eb[ek + 1]) ++ek;
+                            R const z = R(P.atomicNumber[it.et]
+                                          * P.atomicNumber[ek]);
+                            pfc *= z;
+                            pr1 *= z;
+                            pr3 *= z;
                         }
                         R vexp = R(0);
 #pragma unroll
@@ -1328,7 +1382,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             bool const compactSeg = h.type >= 20;
             bool fast = (h.type != 2) && !compactSeg && (h.shapes == NS);
             while (g1 < ge && sG[g1].type == h.type && sG[g1].rc == h.rc
-                   && g1 - g0 < kMaxSegGroups)
+                   && g1 - g0 < segCap(h.type))
             {
                 fast = fast && (sG[g1].shapes == NS);
                 ++g1;
@@ -1344,7 +1398,8 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 }
                 fcRc = h.rc;
             }
-            if ((h.type == 3 || h.type == 21) && h.rc != bitsRc)
+            if ((h.type == 3 || h.type == 13 || h.type == 21
+                 || h.type == 24) && h.rc != bitsRc)
             {
                 // Narrow-angular validity: k != t, r_ik < rc, r_jk^2 < rc^2.
                 R const rc = R(h.rc), rc2 = R(h.rc2);
@@ -1382,7 +1437,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 }
                 bitsRc = h.rc;
             }
-            if (h.type != 2 && !compactSeg)
+            if (h.type != 2 && h.type != 12 && !compactSeg)
             {
                 // Gaussian factors E(r) = exp(-eta (r - rs)^2) per distinct
                 // (eta, rs) of the element (computed once per atom).
@@ -1404,15 +1459,16 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 }
             }
             __syncwarp();
-            if (h.type == 2)
+            if (h.type == 2 || h.type == 12)
             {
                 if (PATHS & kPathRadial)
-                    radialSegment<R, kGenericChunk>(sG, sM, g0, g1, eb, cnt,
-                                                    W, out, L.derivatives);
+                    radialSegment<R, kGenericChunk>(P, sG, sM, g0, g1, eb,
+                                                    cnt, W, out,
+                                                    L.derivatives);
                 else if (lane == 0)
                     atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
             }
-            else if (h.type == 20)
+            else if (h.type == 20 || h.type == 23)
             {
                 if (PATHS & kPathCompRad)
                     compactRadialSegment<R, kGenericChunk>(
@@ -1420,7 +1476,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 else if (lane == 0)
                     atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
             }
-            else if (h.type == 21)
+            else if (h.type == 21 || h.type == 24)
             {
                 if (PATHS & kPathCompNarrow)
                     compactAngularSegment<R, kCompactChunk, true>(
@@ -1429,7 +1485,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 else if (lane == 0)
                     atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
             }
-            else if (h.type == 22)
+            else if (h.type == 22 || h.type == 25)
             {
                 if (PATHS & kPathCompWide)
                     compactAngularSegment<R, kCompactChunk, false>(
@@ -1456,7 +1512,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 else if (lane == 0)
                     atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
             }
-            else if (h.type == 3)
+            else if (h.type == 3 || h.type == 13)
             {
                 if (PATHS & kPathGenNarrow)
                     angularGeneric<R, CT, kGenericChunk, true>(
@@ -1491,7 +1547,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 }
 
 // Paths a potential needs for shape count NS: the kernel's own segment
-// rule (consecutive groups of equal (type, rc), at most kMaxSegGroups; fast
+// rule (consecutive groups of equal (type, rc), at most segCap(type); fast
 // only if every group of the segment has NS shapes).
 inline int pathsNeeded(SFParams const& P, int NS)
 {
@@ -1506,18 +1562,19 @@ inline int pathsNeeded(SFParams const& P, int NS)
             int g1 = g0 + 1;
             bool fast = (h.type != 2) && (h.type < 20) && (h.shapes == NS);
             while (g1 < ge && P.groups[g1].type == h.type
-                   && P.groups[g1].rc == h.rc && g1 - g0 < kMaxSegGroups)
+                   && P.groups[g1].rc == h.rc && g1 - g0 < segCap(h.type))
             {
                 fast = fast && (P.groups[g1].shapes == NS);
                 ++g1;
             }
-            if (h.type == 2) paths |= kPathRadial;
-            else if (h.type == 20) paths |= kPathCompRad;
-            else if (h.type == 21) paths |= kPathCompNarrow;
-            else if (h.type == 22) paths |= kPathCompWide;
+            if (h.type == 2 || h.type == 12) paths |= kPathRadial;
+            else if (h.type == 20 || h.type == 23) paths |= kPathCompRad;
+            else if (h.type == 21 || h.type == 24) paths |= kPathCompNarrow;
+            else if (h.type == 22 || h.type == 25) paths |= kPathCompWide;
             else if (fast) paths |= (h.type == 3) ? kPathFastNarrow
                                                   : kPathFastWide;
-            else paths |= (h.type == 3) ? kPathGenNarrow : kPathGenWide;
+            else paths |= (h.type == 3 || h.type == 13) ? kPathGenNarrow
+                                                        : kPathGenWide;
             g0 = g1;
         }
     }

@@ -27,7 +27,8 @@ enum CompactCore
 // Symmetry-function group (SymGrpExpRad / SymGrpExpAngn / SymGrpExpAngw).
 struct DevGroup
 {
-    int    type;        // 2, 3, 9; compact 20, 21, 22 (rc = the members'
+    int    type;        // 2, 3, 9; weighted 12, 13 (e1 = e2 = -1: every
+                        // element); compact 20, 21, 22 (rc = the members'
                         // largest rc, SymGrpBaseComp::rmax)
     int    e1, e2;      // neighbor elements (e2 == -1: radial)
     int    mbeg, mcnt;  // member range
@@ -78,6 +79,7 @@ struct SFParams
     int       groupBeg[kMaxElem + 1];
     int       numSF[kMaxElem];
     int       numSlots[kMaxElem][kMaxElem];
+    int       atomicNumber[kMaxElem];  // weights of types 12 and 13
     double    PI, PI_2, E, TANH_PRE;  // CutoffFunction constants, host-made
     DevGroup  groups[kMaxGroups];
     DevMember members[kMaxMembers];

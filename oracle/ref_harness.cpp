@@ -22,9 +22,13 @@
 #include "SymFnc.h"
 #include "SymFncBaseComp.h"
 #include "SymFncBaseCompAng.h"
+#include "SymFncBaseCompAngWeighted.h"
 #include "SymFncBaseExpAng.h"
 #include "SymFncCompRad.h"
+#include "SymFncCompRadWeighted.h"
+#include "SymFncExpAngnWeighted.h"
 #include "SymFncExpRad.h"
+#include "SymFncExpRadWeighted.h"
 #include "utility.h"
 
 #include <chrono>
@@ -210,6 +214,26 @@ int refh_sf_params(void* p, int e, int s, double* out)
         out[7] = a->getLambda();
         return 0;
     }
+    if (auto w = dynamic_cast<SymFncExpRadWeighted const*>(&f))
+    {
+        out[1] = -1.0;
+        out[2] = -1.0;
+        out[3] = w->getEta();
+        out[4] = w->getRs();
+        out[6] = 0.0;
+        out[7] = 0.0;
+        return 0;
+    }
+    if (auto w = dynamic_cast<SymFncExpAngnWeighted const*>(&f))
+    {
+        out[1] = -1.0;
+        out[2] = -1.0;
+        out[3] = w->getEta();
+        out[4] = w->getRs();
+        out[6] = w->getZeta();
+        out[7] = w->getLambda();
+        return 0;
+    }
     if (auto c = dynamic_cast<SymFncBaseComp const*>(&f))
     {
         // Compact types: rl, subtype rank in string order (e, p1, p1a, p2,
@@ -232,6 +256,20 @@ int refh_sf_params(void* p, int e, int s, double* out)
         {
             out[1] = (double)a->getE1();
             out[2] = (double)a->getE2();
+            out[6] = a->getAngleLeft();
+            out[7] = a->getAngleRight();
+            return 0;
+        }
+        if (dynamic_cast<SymFncCompRadWeighted const*>(&f))
+        {
+            out[1] = -1.0;
+            out[2] = -1.0;
+            return 0;
+        }
+        if (auto a = dynamic_cast<SymFncBaseCompAngWeighted const*>(&f))
+        {
+            out[1] = -1.0;
+            out[2] = -1.0;
             out[6] = a->getAngleLeft();
             out[7] = a->getAngleRight();
             return 0;

@@ -16,9 +16,10 @@ weights.008.data, scaling.data} for
   (rl, rc), which exercises the reuse of the r_jk radial value in
   SymGrpCompAngn; plus a few types 2 and 3 so that the compact paths run
   beside the Gaussian ones.  48 SFs, NN 48-20-20-1 (tanh, tanh, linear);
-* h2o_wtd -- the element-weighted Gaussian family: types 12 and 13
-  (weights: atomic numbers), with rs = 0 and rs > 0 members, beside a few
-  types 2 and 3.  21 SFs, NN 21-15-15-1 (tanh, tanh, linear).
+* h2o_wtd -- the element-weighted families: Gaussian types 12 and 13
+  (weights: atomic numbers) with rs = 0 and rs > 0 members, and compact
+  types 23, 24 and 25, beside a few types 2 and 3.  29 SFs, NN 29-15-15-1
+  (tanh, tanh, linear).
 
     python tests/golden/make_potentials.py [name ...]   # default: all
 
@@ -109,6 +110,13 @@ def wtd_lines():
                     lines.append(f"symfunction_short {ec} 13 {eta} 0.0 "
                                  f"{lam} {zeta} 12.0")
         lines.append(f"symfunction_short {ec} 13 0.02 1.0 1.0 2.0 12.0")
+        for st, rl, rc in (("p2", 0.0, 12.0), ("p3a", 1.0, 7.0),
+                           ("e", 0.0, 9.0)):
+            lines.append(f"symfunction_short {ec} 23 {rl} {rc} {st}")
+        for al, ar in ((0.0, 100.0), (80.0, 180.0), (-40.0, 40.0)):
+            lines.append(f"symfunction_short {ec} 24 0.0 11.0 {al} {ar} p2")
+        for al, ar in ((30.0, 150.0), (0.0, 180.0)):
+            lines.append(f"symfunction_short {ec} 25 0.0 9.0 {al} {ar} p4")
         for e1 in ELEMENTS:
             for eta in (0.01, 0.1):
                 lines.append(f"symfunction_short {ec} 2 {e1} {eta} 0.0 12.0")
