@@ -192,6 +192,9 @@ struct n2p2b_context
     bool         weighted = false;
     bool         tablesReady = false;
     SFParams     sfp{};
+    std::vector<DevGroup>  tabGroups;    // SF tables (sfp points here)
+    std::vector<DevMember> tabMembers;
+    DevBuf       tabGroupsDev, tabMembersDev;
     NNParams     nnp{};
     int          maxSF = 0;
     int          maxSlots = 0;
@@ -361,7 +364,8 @@ struct n2p2b_context
                           &nbrCountElem, &nbrOff, &keyTmp, &key, &nbrIdx,
                           &nbrEl, &dx, &dy, &dz, &dd, &entryAtom, &mirror,
                           &pairF, &dGdr, &G, &dEdG, &dGdrSelf, &Ei, &selfF,
-                          &F, &energyOut, &status})
+                          &F, &energyOut, &status, &tabGroupsDev,
+                          &tabMembersDev})
             b->release();
         if (statusHost) cudaFreeHost(statusHost);
         if (energyHost) cudaFreeHost(energyHost);
@@ -464,6 +468,16 @@ struct n2p2b_context
             throw std::runtime_error("ERROR: Too many symmetry functions per "
                                      "element for the device tables.\n");
         std::memset(&sfp, 0, sizeof(sfp));
+        {
+            std::size_t ng = 0, nm = 0;
+            for (auto const& el : pot.elements)
+            {
+                ng += el.groups.size();
+                for (auto const& g : el.groups) nm += g.members.size();
+            }
+            tabGroups.assign(ng, DevGroup{});
+            tabMembers.assign(nm, DevMember{});
+        }
         sfp.numElements = ne;
         sfp.cutoffType = pot.cutoffType;
         sfp.maxSlots = maxSlots;
@@ -498,12 +512,7 @@ struct n2p2b_context
             }
             for (auto const& g : el.groups)
             {
-                if (gi >= kMaxGroups || mi + (int)g.members.size()
-                                        > kMaxMembers)
-                    throw std::runtime_error("ERROR: Too many symmetry "
-                                             "function groups/members for "
-                                             "the device tables.\n");
-                DevGroup& d = sfp.groups[gi++];
+                DevGroup& d = tabGroups[gi++];
                 d.type = g.type;
                 d.e1 = g.e1;
                 d.e2 = g.e2;
@@ -518,7 +527,7 @@ struct n2p2b_context
                 for (std::size_t k = 0; k < g.members.size(); ++k)
                 {
                     SymFnc const& s = el.sfs[g.members[k]];
-                    DevMember& m = sfp.members[mi++];
+                    DevMember& m = tabMembers[mi++];
                     std::memset(&m, 0, sizeof(m));
                     m.eta = s.eta;
                     m.rs = s.rs;
@@ -627,6 +636,19 @@ struct n2p2b_context
             sfp.maxExp = std::max(sfp.maxExp, expCount);
         }
         sfp.groupBeg[ne] = gi;
+        sfp.numGroups = gi;
+        sfp.numMembers = mi;
+        sfp.groups = tabGroups.data();
+        sfp.members = tabMembers.data();
+        // Tables up to 32 KB are staged in shared memory by the kernels;
+        // N2P2B_SF_GLOBAL_TABLES=1 keeps them in global memory (tests).
+        {
+            std::size_t const b = sizeof(DevGroup) * tabGroups.size()
+                                + sizeof(DevMember) * tabMembers.size();
+            char const* env = std::getenv("N2P2B_SF_GLOBAL_TABLES");
+            sfp.stageTables = (b <= 32 * 1024
+                               && !(env && std::atoi(env) != 0)) ? 1 : 0;
+        }
 
         // NN blob.
         std::vector<double> blob;
@@ -643,6 +665,20 @@ struct n2p2b_context
             return;
         }
         activate();
+        tabGroupsDev.ensure(sizeof(DevGroup) * std::max<std::size_t>(
+                                tabGroups.size(), 1));
+        tabMembersDev.ensure(sizeof(DevMember) * std::max<std::size_t>(
+                                 tabMembers.size(), 1));
+        if (!tabGroups.empty())
+            ck(cudaMemcpy(tabGroupsDev.p, tabGroups.data(),
+                          sizeof(DevGroup) * tabGroups.size(),
+                          cudaMemcpyHostToDevice), "copy SF groups");
+        if (!tabMembers.empty())
+            ck(cudaMemcpy(tabMembersDev.p, tabMembers.data(),
+                          sizeof(DevMember) * tabMembers.size(),
+                          cudaMemcpyHostToDevice), "copy SF members");
+        sfp.dGroups = tabGroupsDev.as<DevGroup>();
+        sfp.dMembers = tabMembersDev.as<DevMember>();
         sfScale.ensure(sizeof(SFScale) * scale.size());
         ck(cudaMemcpy(sfScale.p, scale.data(), sizeof(SFScale) * scale.size(),
                       cudaMemcpyHostToDevice), "copy SF scaling");

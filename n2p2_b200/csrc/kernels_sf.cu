@@ -38,10 +38,7 @@ long warpBytesFor(SFParams const& P, int cap, int precision)
 
 std::size_t sfSharedBytes(SFParams const& P, int cap, int precision)
 {
-    int const ng = P.groupBeg[P.numElements];
-    int nm = 0;
-    if (ng > 0) nm = P.groups[ng - 1].mbeg + P.groups[ng - 1].mcnt;
-    return sfk::tableBytes(ng, nm)
+    return sfk::stagedTableBytes(P)
          + (std::size_t)sfk::kWarps * warpBytesFor(P, cap, precision);
 }
 

@@ -69,10 +69,17 @@ namespace sfk
 
 constexpr int kWarps = 4;                 // warps (atoms) per CTA
 
-// Bytes of the block-shared group + member tables (16-byte padded).
+// Bytes of the block-shared group + member tables (16-byte padded); tables
+// above kMaxTableBytes stay in global memory (read through L1) instead
+// (SFParams::stageTables, set by the host).
+constexpr std::size_t kMaxTableBytes = 32 * 1024;
 __host__ __device__ inline std::size_t tableBytes(int ng, int nm)
 {
     return ((ng * sizeof(DevGroup) + nm * sizeof(DevMember) + 15) / 16) * 16;
+}
+__host__ __device__ inline std::size_t stagedTableBytes(SFParams const& P)
+{
+    return P.stageTables ? tableBytes(P.numGroups, P.numMembers) : 0;
 }
 constexpr int kThreads = 32 * kWarps;
 // Members per register chunk of the general paths; small so that their
@@ -1285,27 +1292,34 @@ __global__ void __launch_bounds__(kThreads,
 sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 {
     extern __shared__ double smem0[];
-    // Block-shared copy of the group and member tables (dynamically indexed
-    // reads from the parameter bank measured ~25% slower overall).
-    int const ng = P.groupBeg[P.numElements];
-    int nm = 0;
-    if (ng > 0) nm = P.groups[ng - 1].mbeg + P.groups[ng - 1].mcnt;
-    DevGroup* tg = reinterpret_cast<DevGroup*>(smem0);
-    DevMember* tm = reinterpret_cast<DevMember*>(tg + ng);
+    // Block-shared copy of the group and member tables when they fit
+    // (dynamically indexed reads from global memory measured ~25% slower
+    // overall); larger tables are read from global memory through L1.
+    int const ng = P.numGroups;
+    int const nm = P.numMembers;
+    // Only the all-paths instantiation may read the tables from global
+    // memory; the others see shared-memory pointers (LDS in the hot loops).
+    bool const stage = (PATHS != kPathAll) || P.stageTables;
+    std::size_t const staged = stage ? tableBytes(ng, nm) : 0;
+    DevGroup const* sG = P.dGroups;
+    DevMember const* sM = P.dMembers;
+    if (stage)
     {
-        int const* src = reinterpret_cast<int const*>(P.groups);
+        DevGroup* tg = reinterpret_cast<DevGroup*>(smem0);
+        DevMember* tm = reinterpret_cast<DevMember*>(tg + ng);
+        int const* src = reinterpret_cast<int const*>(P.dGroups);
         int* dst = reinterpret_cast<int*>(tg);
         int const words = (int)(ng * sizeof(DevGroup) / sizeof(int));
         for (int k = threadIdx.x; k < words; k += kThreads) dst[k] = src[k];
-        src = reinterpret_cast<int const*>(P.members);
+        src = reinterpret_cast<int const*>(P.dMembers);
         dst = reinterpret_cast<int*>(tm);
         int const wm = (int)(nm * sizeof(DevMember) / sizeof(int));
         for (int k = threadIdx.x; k < wm; k += kThreads) dst[k] = src[k];
+        sG = tg;
+        sM = tm;
     }
     __syncthreads();
-    char* smem = reinterpret_cast<char*>(smem0) + tableBytes(ng, nm);
-    DevGroup const* sG = tg;
-    DevMember const* sM = tm;
+    char* smem = reinterpret_cast<char*>(smem0) + staged;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
 
     int const lane = threadIdx.x & 31;
@@ -1589,7 +1603,8 @@ constexpr int kPathsCommon = kPathRadial | kPathFastNarrow;
 inline bool useCommonPaths(SFParams const& P, int NS)
 {
     int const need = pathsNeeded(P, NS);
-    return (need & ~kPathsCommon) == 0 && L_pathsOverride() != kPathAll;
+    return (need & ~kPathsCommon) == 0 && P.stageTables
+        && L_pathsOverride() != kPathAll;
 }
 
 template <typename R, int CT, int NS, int NRC>

@@ -1,7 +1,8 @@
 // Plain-old-data parameter tables shared by the host builder (context.cu) and
-// the kernels.  They are passed to kernels by value as __grid_constant__
-// parameters, so every potential parameter a warp reads uniformly is served
-// from the constant bank (no load instruction, no shared-memory staging).
+// the kernels.  The scalar parameters go to kernels by value as
+// __grid_constant__ parameters; the symmetry-function group and member
+// tables live in device memory (any size) and the kernel stages them into
+// shared memory when they fit.
 #pragma once
 
 #include <cstdint>
@@ -10,11 +11,9 @@ namespace n2p2b
 {
 
 constexpr int kMaxElem      = 6;    // elements per potential on the device
-constexpr int kMaxGroups    = 48;   // SF groups, all elements together
-constexpr int kMaxMembers   = 256;  // SF group members, all elements
-constexpr int kMaxSF        = 256;  // symmetry functions per element
+constexpr int kMaxSF        = 4096; // symmetry functions per element
 constexpr int kMaxLayers    = 8;    // NN layers incl. input and output
-constexpr int kMaxWidth     = 256;  // NN layer width
+constexpr int kMaxWidth     = 512;  // NN layer width
 
 // Core functions of the compact symmetry functions (CoreFunction::Type,
 // libnnp/CoreFunction.h), as subtypes "p1".."p4" (optionally "a":
@@ -81,8 +80,15 @@ struct SFParams
     int       numSlots[kMaxElem][kMaxElem];
     int       atomicNumber[kMaxElem];  // weights of types 12 and 13
     double    PI, PI_2, E, TANH_PRE;  // CutoffFunction constants, host-made
-    DevGroup  groups[kMaxGroups];
-    DevMember members[kMaxMembers];
+    int       numGroups;
+    int       numMembers;
+    int       stageTables;     // 1: kernels copy the tables to shared memory
+    // Group / member tables: host copies (launch analysis on the host) and
+    // device copies (kernels), same contents.
+    DevGroup const*  groups;
+    DevMember const* members;
+    DevGroup const*  dGroups;
+    DevMember const* dMembers;
 };
 
 // Final G transform per SF: G = Smin + b * (q * v - shift), with

@@ -120,3 +120,19 @@ def test_family_mixed_form_accuracy(gpu, name):
           f"F RMSE {f_rmse:.2e} (F rms {f_rms:.2e})")
     assert e_rmse <= 1e-4 * e_scale
     assert f_rmse <= 1e-2 * f_rms
+
+
+@pytest.mark.parametrize("name", FAMILIES)
+def test_family_global_tables(gpu, name, monkeypatch):
+    """Potentials whose group tables exceed the shared-memory budget (the
+    reference's own polynomial examples have up to 354 SFs per element)
+    read them from global memory; forced here on a small potential."""
+    monkeypatch.setenv("N2P2B_SF_GLOBAL_TABLES", "1")
+    p, ref = _models(name)
+    box, pos, elem = synth.water_box(64, 17)
+    ref.set_structure(pos, elem, box)
+    e0, f0 = ref.predict()
+    e1, f1 = p.predict(pos, elem, box)
+    assert abs(e1 - e0) <= 1e-10 * abs(e0)
+    scale = np.maximum(np.abs(f0), np.sqrt(np.mean(f0 ** 2)))
+    assert np.all(np.abs(f1 - f0) <= 1e-10 * scale)

@@ -24,7 +24,8 @@ def potential_dirs():
     out = [os.path.join(POT, d) for d in sorted(os.listdir(POT))
            if os.path.exists(os.path.join(POT, d, "input.nn"))]
     if reference_tree_available():
-        for name in ("H2O_RPBE-D3", "Cu2S_PBE"):
+        for name in ("H2O_RPBE-D3", "Cu2S_PBE", "Ethylbenzene_SCAN",
+                     "DMABN_SCAN", "Anisole_SCAN"):
             out.append(os.path.join(REFERENCE, "examples", "nnp-predict",
                                     name))
     return out
