@@ -771,6 +771,140 @@ __global__ void nlbMirrorKernel(int n, int NIMG,
     }
 }
 
+// Batch neighbor list, faster form of nlbBruteKernel for structures with at
+// most 128 images (|bc| <= 2 per box vector): warp per atom i, lanes over
+// the candidates j of one element (positions loaded once), each lane walks
+// the structure's images in key order with an incremental (b0, b1, b2)
+// counter.  An FP32 distance test only filters: its threshold rc^2 + m
+// covers the FP32 rounding of the displacement and image-shift sums (m from
+// a bound on their magnitudes, at least 1e-4 rc^2), and every candidate it
+// keeps gets the exact FP64 test of nlTest, so the neighbor sets are those
+// of the brute path.  Hits are kept
+// as per-lane image bit masks and written in key order (lane = j
+// ascending, bits = image ascending) through a warp prefix sum.
+template <int MODE>
+__global__ void nlbLaneKernel(int n, int numElements, int NIMG,
+                              double const* __restrict__ pos,
+                              int const* __restrict__ structOf,
+                              BatchStruct const* __restrict__ bs,
+                              int const* __restrict__ structAtoms,
+                              int* __restrict__ nbrCount,
+                              int* __restrict__ nbrCountElem,
+                              int const* __restrict__ nbrOff,
+                              unsigned long long* __restrict__ key,
+                              int const* __restrict__ status)
+{
+    if (status[ST_FLAGS] & FLAG_ABORT) return;
+    int const lane = threadIdx.x & 31;
+    int const i = (int)((blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5);
+    if (i >= n) return;
+    BatchStruct const& S = bs[structOf[i]];
+    NLParams const& p = S.p;
+    int const nimg = p.nimg;
+    int const q0 = p.periodic ? p.pbc[0] : 0;
+    int const q1 = p.periodic ? p.pbc[1] : 0;
+    int const q2 = p.periodic ? p.pbc[2] : 0;
+    float a[3][3];
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) a[r][c] = (float)p.box[r][c];
+    double const ri[3] = {pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]};
+    // Largest image shift per component: sum_r |pbc_r a_r|.
+    float shiftMax = 0.0f;
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+        shiftMax = fmaxf(shiftMax, fabsf(a[0][c]) * q0 + fabsf(a[1][c]) * q1
+                                   + fabsf(a[2][c]) * q2);
+    float const rcf = sqrtf((float)p.rc2);
+    int total = 0;
+    long const base = (MODE == 1) ? (long)nbrOff[i] : 0;
+    for (int e = 0; e < numElements; ++e)
+    {
+        int const eb = S.es[e];
+        int const ne = S.es[e + 1] - eb;
+        int cntE = 0;
+        for (int j0 = 0; j0 < ne; j0 += 32)
+        {
+            int const jj = j0 + lane;
+            unsigned mask[4] = {0u, 0u, 0u, 0u};
+            int j = 0;
+            if (jj < ne)
+            {
+                j = structAtoms[eb + jj];
+                float const d0 = (float)(ri[0] - pos[3 * j + 0]);
+                float const d1 = (float)(ri[1] - pos[3 * j + 1]);
+                float const d2 = (float)(ri[2] - pos[3 * j + 2]);
+                // Per component the FP32 sum of up to four terms of size
+                // <= M errs by < 8 M 2^-24 (rounded box included); r^2
+                // near the cutoff then errs by < 2 rc 3 e + 3 e^2.
+                float const M = fmaxf(fmaxf(fabsf(d0), fabsf(d1)), fabsf(d2))
+                              + shiftMax;
+                float const err = 8.0f * M * 5.9604645e-8f;
+                float const rc2f = (float)p.rc2
+                                 + fmaxf(1e-4f * (float)p.rc2,
+                                         4.0f * (6.0f * rcf * err
+                                                 + 3.0f * err * err));
+                int b0 = -q0, b1 = -q1, b2 = -q2;
+                for (int img = 0; img < nimg; ++img)
+                {
+                    float const x = d0 + b0 * a[0][0] + b1 * a[1][0]
+                                  + b2 * a[2][0];
+                    float const y = d1 + b0 * a[0][1] + b1 * a[1][1]
+                                  + b2 * a[2][1];
+                    float const z = d2 + b0 * a[0][2] + b1 * a[1][2]
+                                  + b2 * a[2][2];
+                    if (x * x + y * y + z * z <= rc2f
+                        && !(j == i && b0 == 0 && b1 == 0 && b2 == 0))
+                    {
+                        double dr[3];
+                        if (nlTest(p, ri, pos, j, b0, b1, b2, dr))
+                            mask[img >> 5] |= 1u << (img & 31);
+                    }
+                    if (++b2 > q2)
+                    {
+                        b2 = -q2;
+                        if (++b1 > q1)
+                        {
+                            b1 = -q1;
+                            ++b0;
+                        }
+                    }
+                }
+            }
+            int const c = __popc(mask[0]) + __popc(mask[1]) + __popc(mask[2])
+                        + __popc(mask[3]);
+            int incl = c;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1)
+            {
+                int const v = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += v;
+            }
+            int const sum = __shfl_sync(0xffffffffu, incl, 31);
+            if (MODE == 1 && c > 0)
+            {
+                int off = total + incl - c;
+                for (int w = 0; w < 4; ++w)
+                {
+                    unsigned m = mask[w];
+                    while (m)
+                    {
+                        int const img = (w << 5) + __ffs(m) - 1;
+                        m &= m - 1;
+                        key[base + off++] = nlKey(e, j, img, n, NIMG);
+                    }
+                }
+            }
+            total += sum;
+            cntE += sum;
+        }
+        if (MODE == 0 && lane == 0)
+            nbrCountElem[(long)i * numElements + e] = cntE;
+    }
+    if (MODE == 0 && lane == 0) nbrCount[i] = total;
+}
+
 void launchNeighborListBatch(NLBatchLaunch const& L, cudaStream_t s)
 {
     int const n = L.n;
@@ -780,14 +914,34 @@ void launchNeighborListBatch(NLBatchLaunch const& L, cudaStream_t s)
     int const gWarp = (n + wpb - 1) / wpb;
     nlbPrepareKernel<<<gAtoms, tb, 0, s>>>(n, L.posIn, L.structOf, L.bs,
                                            L.normalize, L.convLength, L.pos);
-    nlbBruteKernel<0><<<gWarp, 32 * wpb, 0, s>>>(
-        n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs, L.structAtoms,
-        L.nbrCount, L.nbrCountElem, L.nbrOff, L.key, L.status);
-    nlScanKernel<<<1, 1024, 0, s>>>(n, L.nbrCount, L.nbrOff, L.capacity,
-                                    L.status);
-    nlbBruteKernel<1><<<gWarp, 32 * wpb, 0, s>>>(
-        n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs, L.structAtoms,
-        L.nbrCount, L.nbrCountElem, L.nbrOff, L.key, L.status);
+    // Structures with more than 128 images (boxes below rc / 2) take the
+    // plain brute path.
+    if (L.NIMG <= 128)
+    {
+        nlbLaneKernel<0><<<gWarp, 32 * wpb, 0, s>>>(
+            n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs,
+            L.structAtoms, L.nbrCount, L.nbrCountElem, L.nbrOff, L.key,
+            L.status);
+        nlScanKernel<<<1, 1024, 0, s>>>(n, L.nbrCount, L.nbrOff, L.capacity,
+                                        L.status);
+        nlbLaneKernel<1><<<gWarp, 32 * wpb, 0, s>>>(
+            n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs,
+            L.structAtoms, L.nbrCount, L.nbrCountElem, L.nbrOff, L.key,
+            L.status);
+    }
+    else
+    {
+        nlbBruteKernel<0><<<gWarp, 32 * wpb, 0, s>>>(
+            n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs,
+            L.structAtoms, L.nbrCount, L.nbrCountElem, L.nbrOff, L.key,
+            L.status);
+        nlScanKernel<<<1, 1024, 0, s>>>(n, L.nbrCount, L.nbrOff, L.capacity,
+                                        L.status);
+        nlbBruteKernel<1><<<gWarp, 32 * wpb, 0, s>>>(
+            n, L.numElements, L.NIMG, L.pos, L.structOf, L.bs,
+            L.structAtoms, L.nbrCount, L.nbrCountElem, L.nbrOff, L.key,
+            L.status);
+    }
     nlbFinishKernel<<<gWarp, 32 * wpb, 0, s>>>(
         n, L.NIMG, L.pos, L.elem, L.structOf, L.bs, L.nbrOff, L.key,
         L.nbrIdx, L.nbrEl, L.dx, L.dy, L.dz, L.dd, L.status);
