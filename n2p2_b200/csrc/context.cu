@@ -248,7 +248,7 @@ struct n2p2b_context
         long               step = 0;         // Adam steps taken
         int                maxH = 0, maxNin = 0, maxParams = 0;
         DevBuf             w, m, v, grad, gpart, rE, rF, u, loss, dRange,
-                           list, listCount;
+                           list, listCount, lrScale;
     } stu;
 
     // Structure.
@@ -1407,6 +1407,7 @@ struct n2p2b_context
         std::swap(s.dRange, stu.dRange);
         std::swap(s.list, stu.list);
         std::swap(s.listCount, stu.listCount);
+        std::swap(s.lrScale, stu.lrScale);
         stu = std::move(s);
         if (hostOnly()) return;
         activate();
@@ -1418,6 +1419,24 @@ struct n2p2b_context
         ck(cudaMemcpy(stu.dRange.p, stu.range.data(),
                       sizeof(Range) * stu.range.size(),
                       cudaMemcpyHostToDevice), "copy training range");
+        // Adam's W1 learning-rate factors: 1 / sigma of each input
+        // (scaling.data), sigma floored at 1e-3 of the element's largest.
+        {
+            std::vector<float> lrs((std::size_t)ne * maxSF, 1.0f);
+            for (int e = 0; e < ne; ++e)
+            {
+                auto const& sfs = stu.pot.elements[e].sfs;
+                double smax = 0.0;
+                for (auto const& f : sfs) smax = std::max(smax, f.Gsigma);
+                if (!(smax > 0.0)) continue;
+                for (auto const& f : sfs)
+                    lrs[(std::size_t)e * maxSF + f.index] =
+                        (float)(1.0 / std::max(f.Gsigma, 1e-3 * smax));
+            }
+            stu.lrScale.ensure(sizeof(float) * lrs.size());
+            ck(cudaMemcpy(stu.lrScale.p, lrs.data(), sizeof(float) * lrs.size(),
+                          cudaMemcpyHostToDevice), "copy learning rates");
+        }
         stu.listCount.ensure(sizeof(int) * kMaxElem);
         stu.loss.ensure(sizeof(double) * 2);
         if (n > 0) stu.list.ensure(sizeof(int) * n);
@@ -1624,6 +1643,7 @@ struct n2p2b_context
         S.gpart = stu.gpart.as<float>();
         S.grad = stu.grad.as<float>();
         S.loss = stu.loss.as<double>();
+        S.lrScale = stu.lrScale.as<float>();
         S.lr = (float)lr;
         ++stu.step;
         S.bc1 = (float)(1.0 - std::pow((double)S.beta1, (double)stu.step));

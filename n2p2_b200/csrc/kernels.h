@@ -295,6 +295,9 @@ struct StudentLaunch
     int            numSF[kMaxElem] = {};
     int            numSlots[kMaxElem][kMaxElem] = {};
     int            hidden[kMaxElem] = {};
+    // Adam learning-rate factor per (element, input): 1 / sigma of the
+    // input symmetry function (Adam on W1 for standardized inputs).
+    float const*   lrScale = nullptr;         // [numElements][maxSF]
     long           woff1[kMaxElem] = {}, wtoff1[kMaxElem] = {};
     long           boff1[kMaxElem] = {};
     long           woff2[kMaxElem] = {}, wtoff2[kMaxElem] = {};

@@ -25,7 +25,9 @@
 // Kernels: residuals of the batch atoms; the adjoint (warp per atom j over
 // its neighbor entries, the layout of the force kernel); per-block partial
 // gradients (64 atoms of one element per block); a fixed-order reduction of
-// the partials fused with the Adam update (Kingma & Ba, bias-corrected); and
+// the partials fused with the Adam update (Kingma & Ba, bias-corrected; the
+// W1 learning rate is divided per input by that symmetry function's sigma,
+// i.e. Adam on the weights of standardized inputs G / sigma); and
 // the training range of the symmetry functions (per-SF min / max of the
 // unscaled values) that gates the student at inference.
 #include <cfloat>
@@ -232,11 +234,13 @@ __global__ void adamKernel(StudentLaunch const L)
     for (int b = L.blkBeg[e]; b < L.blkBeg[e + 1]; ++b)
         g += L.gpart[(long)b * L.paramStride + p];
     long pos, posT = -1;
+    float lr = L.lr;
     if (p < nW)
     {
         int const k = p / nin, l = p - (p / nin) * nin;
         pos = L.woff1[e] + p;
         posT = L.wtoff1[e] + (long)l * H + k;
+        if (L.lrScale) lr *= L.lrScale[(long)e * L.maxSF + l];
     }
     else if (p < nW + H) pos = L.boff1[e] + (p - nW);
     else if (p < nW + 2 * H)
@@ -252,7 +256,7 @@ __global__ void adamKernel(StudentLaunch const L)
     L.v[pos] = v;
     float const mh = m / L.bc1;
     float const vh = v / L.bc2;
-    float const w = L.blob[pos] - L.lr * mh / (sqrtf(vh) + L.epsAdam);
+    float const w = L.blob[pos] - lr * mh / (sqrtf(vh) + L.epsAdam);
     L.blob[pos] = w;
     if (posT >= 0) L.blob[posT] = w;
 }

@@ -47,7 +47,10 @@ def make_student_dir(teacher_dir: str, out_dir: str, num_sf: dict[str, int],
                      energy_bias: dict[str, float] | None = None):
     """Writes input.nn (the teacher's, with a 1-hidden-layer tanh network),
     the teacher's scaling.data and seeded initial weights (normal, variance
-    1 / fan-in; output bias = the element's mean label energy)."""
+    1 / fan-in for standardized inputs: column l of W1 divided by sigma_l
+    of scaling.data, floored at 1e-3 of the element's largest; output bias
+    = the element's mean label energy).  Training then runs Adam on the
+    standardized weights (per-input learning rate lr / sigma_l)."""
     os.makedirs(out_dir, exist_ok=True)
     lines = []
     with open(os.path.join(teacher_dir, "input.nn")) as fh:
@@ -64,9 +67,21 @@ def make_student_dir(teacher_dir: str, out_dir: str, num_sf: dict[str, int],
         fh.write("\n".join(lines) + "\n")
     shutil.copyfile(os.path.join(teacher_dir, "scaling.data"),
                     os.path.join(out_dir, "scaling.data"))
+    sigma = {}
+    with open(os.path.join(teacher_dir, "scaling.data")) as fh:
+        for ln in fh:
+            w = ln.split()
+            if len(w) < 6 or w[0].startswith("#"):
+                continue
+            sigma.setdefault(int(w[0]), {})[int(w[1])] = float(w[5])
+    syms = sorted(num_sf, key=atomic_number)
     rng = np.random.default_rng(seed)
     for sym, nin in num_sf.items():
         W1 = rng.normal(0.0, 1.0 / np.sqrt(nin), (hidden, nin))
+        sg = sigma.get(syms.index(sym) + 1, {})
+        if sg:
+            sv = np.array([sg.get(l + 1, 1.0) for l in range(nin)])
+            W1 /= np.maximum(sv, 1e-3 * sv.max())[None, :]
         b1 = np.zeros(hidden)
         w2 = rng.normal(0.0, 1.0 / np.sqrt(hidden), hidden)
         b2 = (energy_bias or {}).get(sym, 0.0)
@@ -121,8 +136,11 @@ def label_frames(teacher_dir: str, frames, elem, device: int = 0):
 def train(teacher_dir: str, student_dir: str, frames, elem, labels,
           epochs: int = 20, batch: int = 4096, lr: float = 1e-3,
           w_energy: float = 1.0, w_force: float = 1.0, seed: int = 11,
-          device: int = 0, log=print):
-    """Trains the student in `student_dir` in place and writes it back."""
+          device: int = 0, log=print, lr_final: float | None = None,
+          decay_epochs: int = 5):
+    """Trains the student in `student_dir` in place and writes it back.
+    With `lr_final`, the learning rate stays `lr` and then falls linearly
+    to `lr_final` over the last `decay_epochs` epochs."""
     import torch
     from .mode import Prediction
     E, Fo = labels
@@ -139,6 +157,10 @@ def train(teacher_dir: str, student_dir: str, frames, elem, labels,
     p.student_update_range(reset=True)
     history = []
     for ep in range(epochs):
+        lr_ep = lr
+        if lr_final is not None and ep >= epochs - decay_epochs:
+            f = (ep - (epochs - decay_epochs) + 1) / decay_epochs
+            lr_ep = lr + (lr_final - lr) * f
         order = rng.permutation(len(frames))
         le = lf = 0.0
         cnt = 0
@@ -155,7 +177,7 @@ def train(teacher_dir: str, student_dir: str, frames, elem, labels,
                 idx = perm[b0:b0 + batch].contiguous()
                 want = b0 + batch >= n
                 r = p.student_train_step(E[fi], Fo[fi], idx, w_energy,
-                                         w_force, lr, want_loss=want)
+                                         w_force, lr_ep, want_loss=want)
                 steps += 1
                 if r is not None:
                     le += r[0]
@@ -172,7 +194,8 @@ def train(teacher_dir: str, student_dir: str, frames, elem, labels,
 
 
 def distill(teacher_dir: str, out_dir: str, n_frames=500, epochs=20,
-            batch=4096, lr=1e-3, hidden=16, seed=0, device=0, log=print):
+            batch=4096, lr=1e-3, hidden=16, seed=0, device=0, log=print,
+            lr_final=None, w_energy=1.0, w_force=1.0):
     from .mode import Prediction
     frames, elem = training_frames(n_frames)
     log(f"labelling {len(frames)} frames with the FP64 teacher")
@@ -186,7 +209,8 @@ def distill(teacher_dir: str, out_dir: str, n_frames=500, epochs=20,
     host.close()
     make_student_dir(teacher_dir, out_dir, num_sf, hidden, seed, bias)
     return train(teacher_dir, out_dir, frames, elem, labels, epochs, batch,
-                 lr, device=device, log=log)
+                 lr, w_energy, w_force, device=device, log=log,
+                 lr_final=lr_final)
 
 
 def main():
@@ -201,9 +225,15 @@ def main():
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--hidden", type=int, default=16)
     t.add_argument("--seed", type=int, default=0)
+    t.add_argument("--lr-final", type=float, default=None,
+                   help="decay the learning rate linearly to this value "
+                        "over the last five epochs")
+    t.add_argument("--w-energy", type=float, default=1.0)
+    t.add_argument("--w-force", type=float, default=1.0)
     args = a.parse_args()
     r = distill(args.teacher, args.out, args.frames, args.epochs, args.batch,
-                args.lr, args.hidden, args.seed)
+                args.lr, args.hidden, args.seed, lr_final=args.lr_final,
+                w_energy=args.w_energy, w_force=args.w_force)
     print(f"trained: {r['steps']} steps in {r['seconds']:.0f} s")
 
 
