@@ -54,10 +54,10 @@ POT = os.path.join(POT_DIR, "h2o_52")
 STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
 # DRAM bytes (read + write) of one FP64 symmetry-function launch on this
-# workload: dram__bytes_read.sum + dram__bytes_write.sum = 0.576 + 2.510 GB,
+# workload: dram__bytes_read.sum + dram__bytes_write.sum = 0.570 + 2.500 GB,
 # measured by ncu on the launches of this very bench run (the launch list
 # summarized under profiles/).
-SF_TRAFFIC_BYTES = 3.087e9
+SF_TRAFFIC_BYTES = 3.070e9
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
