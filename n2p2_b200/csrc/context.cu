@@ -632,6 +632,14 @@ struct n2p2b_context
                 d.shapes = (g.type == 2 || g.type == 12 || g.type == 13
                             || isCompactType(g.type))
                          ? 0 : productShapes(el, g);
+                {
+                    int zmax = 0;
+                    for (int mi2 : g.members)
+                        zmax = std::max(zmax, el.sfs[mi2].zetaInt - 1);
+                    int b = 0;
+                    while (b < 31 && (zmax >> b) != 0) ++b;
+                    d.powBits = b;
+                }
             }
             sfp.maxExp = std::max(sfp.maxExp, expCount);
         }

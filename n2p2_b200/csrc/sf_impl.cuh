@@ -248,6 +248,24 @@ __device__ __forceinline__ R powInt(R x, int n)
     return result;
 }
 
+// powInt for 0 <= n < 16 without branches: the same multiplications as
+// the loop above for the bits of n (lanes with different exponents do not
+// diverge).  Used by the product-form path where it measured faster: the
+// 8-shape kernels (zeta up to 16) and FP32.
+template <typename R>
+__device__ __forceinline__ R powInt16(R x, int n)
+{
+    R result = R(1);
+#pragma unroll
+    for (int b = 0; b < 4; ++b)
+    {
+        R const t = result * x;
+        result = ((n >> b) & 1) ? t : result;
+        x *= x;
+    }
+    return result;
+}
+
 // Per-warp shared-memory views.
 template <typename R>
 struct WarpMem
@@ -1212,8 +1230,13 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                         for (int s = 0; s < NS; ++s)
                         {
                             pl[s] = R(1) + lam[s] * costijk;
+                            constexpr bool kFixedPow = (NS == 8)
+                                                    || (sizeof(R) == 4);
                             A[s] = (pl[s] <= R(0)) ? R(0)
-                                                   : powInt(pl[s], zi[s] - 1);
+                                   : (kFixedPow && g.powBits <= 4
+                                      && zi[s] >= 1)
+                                     ? powInt16(pl[s], zi[s] - 1)
+                                     : powInt(pl[s], zi[s] - 1);
                             B[s] = A[s] * pl[s] * pfc;
                             Z1[s] = zl[s] * X1;
                             Z3[s] = zl[s] * X3;

@@ -34,6 +34,8 @@ struct DevGroup
     int    shapes;      // angular product form: members = runs x shapes
                         // (same (zeta, lambda) list per eta run, integer
                         // zeta, rs = 0); 0 = not of that form
+    int    powBits;     // bits of the largest zeta - 1 of the members
+                        // (branch-free integer powers when <= 4)
     double rc, rc2;     // cutoff radius and its square
     double rci, iw;     // CutoffFunction::rci, iw  (alpha-shifted inner cutoff)
     double rcinv;       // 1 / rc
