@@ -145,13 +145,15 @@ gradKernel(StudentLaunch const L)
     float* sB = sA + kGradRows * H;           // beta
     float* sC = sB + kGradRows * H;           // gamma (w2 gradient)
     float* sc = sC + kGradRows * H;           // c per row
-    float* sW = sc + kGradRows;               // W1 [H][nin]
+    float* sW = sc + kGradRows;               // W1 [H][ldw]
+    int const ldw = nin | 1;                  // odd stride: no bank conflicts
     T const* const G = static_cast<T const*>(L.G);
     float const* const wb = L.blob;
     float const* W1 = wb + L.woff1[e];
     float const* b1 = wb + L.boff1[e];
     float const* w2 = wb + L.woff2[e];
-    for (int k = threadIdx.x; k < H * nin; k += blockDim.x) sW[k] = W1[k];
+    for (int q = threadIdx.x; q < H * nin; q += blockDim.x)
+        sW[(q / nin) * ldw + q % nin] = W1[q];
     int const lane = threadIdx.x & 31;
     int const warp = threadIdx.x >> 5;
     for (int r = warp; r < kGradRows; r += blockDim.x >> 5)
@@ -166,27 +168,25 @@ gradKernel(StudentLaunch const L)
     }
     __syncthreads();
     float const cE = (float)(2.0 * L.wE * L.eScale / L.batchSize);
-    if (threadIdx.x < kGradRows)
+    // Thread per (row, neuron): z = W1 G + b1 and a = W1 u.
+    for (int q = threadIdx.x; q < kGradRows * H; q += blockDim.x)
     {
-        int const r = threadIdx.x;
+        int const r = q / H, k = q - (q / H) * H;
         int const atom = r < rows ? L.atomsByElem[row0 + r] : -1;
         float const c = atom >= 0 ? cE * L.rE[atom] : 0.0f;
-        sc[r] = c;
-        for (int k = 0; k < H; ++k)
+        if (k == 0) sc[r] = c;
+        float z = b1[k], a = 0.0f;
+        for (int l = 0; l < nin; ++l)
         {
-            float z = b1[k], a = 0.0f;
-            for (int l = 0; l < nin; ++l)
-            {
-                z += sW[k * nin + l] * sG[r * ld + l];
-                a += sW[k * nin + l] * sU[r * ld + l];
-            }
-            float const h = tanhf(z);
-            float const t = 1.0f - h * h;
-            bool const live = atom >= 0;
-            sA[r * H + k] = live ? w2[k] * t * (c - 2.0f * a * h) : 0.0f;
-            sB[r * H + k] = live ? w2[k] * t : 0.0f;
-            sC[r * H + k] = live ? c * h + a * t : 0.0f;
+            z += sW[k * ldw + l] * sG[r * ld + l];
+            a += sW[k * ldw + l] * sU[r * ld + l];
         }
+        float const h = tanhf(z);
+        float const t = 1.0f - h * h;
+        bool const live = atom >= 0;
+        sA[r * H + k] = live ? w2[k] * t * (c - 2.0f * a * h) : 0.0f;
+        sB[r * H + k] = live ? w2[k] * t : 0.0f;
+        sC[r * H + k] = live ? c * h + a * t : 0.0f;
     }
     __syncthreads();
     float* out = L.gpart + (long)blockIdx.x * L.paramStride;
@@ -320,7 +320,7 @@ std::size_t studentGradSmem(int maxNin, int maxH)
 {
     return sizeof(float) * ((std::size_t)2 * kGradRows * (maxNin + 1)
                             + (std::size_t)3 * kGradRows * maxH + kGradRows
-                            + (std::size_t)maxH * maxNin);
+                            + (std::size_t)maxH * (maxNin | 1));
 }
 
 int studentGradBlocks(ElemStarts const& es, int numElements, int* blkBeg)

@@ -2,6 +2,8 @@
 
     python -m n2p2_b200.student train --teacher DIR --out DIR \
         [--frames 500] [--epochs 20] [--batch 4096] [--lr 1e-3] [--hidden 16]
+        [--lr-final LR] [--decay-epochs 5] [--w-energy 1] [--w-force 1]
+        [--sigma-max S] [--init STUDENT_DIR]
 
 The teacher (an n2p2 potential directory) labels perturbed copies of a water
 box with per-atom energies and forces in FP64.  The student -- one hidden
@@ -102,15 +104,18 @@ def make_student_dir(teacher_dir: str, out_dir: str, num_sf: dict[str, int],
 
 def training_frames(n_frames: int = 500, sigma: float = 0.15,
                     strain: float = 0.03, n_mol: int = 8192,
-                    base_seed: int = 2026, seed: int = 7):
+                    base_seed: int = 2026, seed: int = 7,
+                    sigma_max: float | None = None):
     """Perturbed copies of one water box: Gaussian position noise `sigma`
-    and a random isotropic strain in [-strain, strain] per frame."""
+    (with `sigma_max`, a width drawn per frame from U[sigma, sigma_max]) and
+    a random isotropic strain in [-strain, strain] per frame."""
     box, pos, elem = synth.water_box(n_mol, base_seed)
     rng = np.random.default_rng(seed)
     frames = []
     for _ in range(n_frames):
         s = 1.0 + rng.uniform(-strain, strain)
-        x = pos * s + rng.normal(0.0, sigma, pos.shape)
+        sig = sigma if sigma_max is None else rng.uniform(sigma, sigma_max)
+        x = pos * s + rng.normal(0.0, sig, pos.shape)
         frames.append((box * s, x))
     return frames, elem
 
@@ -195,9 +200,13 @@ def train(teacher_dir: str, student_dir: str, frames, elem, labels,
 
 def distill(teacher_dir: str, out_dir: str, n_frames=500, epochs=20,
             batch=4096, lr=1e-3, hidden=16, seed=0, device=0, log=print,
-            lr_final=None, w_energy=1.0, w_force=1.0):
+            lr_final=None, w_energy=1.0, w_force=1.0, decay_epochs=5,
+            init=None, sigma=0.15, sigma_max=None):
+    """Labels the training frames with the teacher and trains a student in
+    `out_dir`: a fresh one, or with `init` a copy of that student directory
+    (its network and weights) trained further."""
     from .mode import Prediction
-    frames, elem = training_frames(n_frames)
+    frames, elem = training_frames(n_frames, sigma=sigma, sigma_max=sigma_max)
     log(f"labelling {len(frames)} frames with the FP64 teacher")
     labels = label_frames(teacher_dir, frames, elem, device)
     host = Prediction(teacher_dir, device=-1)
@@ -207,10 +216,17 @@ def distill(teacher_dir: str, out_dir: str, n_frames=500, epochs=20,
     Ecpu = labels[0][0].cpu().numpy()
     bias = {s: float(Ecpu[elem == e].mean()) for e, s in enumerate(syms)}
     host.close()
-    make_student_dir(teacher_dir, out_dir, num_sf, hidden, seed, bias)
+    if init is None:
+        make_student_dir(teacher_dir, out_dir, num_sf, hidden, seed, bias)
+    else:
+        os.makedirs(out_dir, exist_ok=True)
+        for f in os.listdir(init):
+            if f != "training.log" and os.path.isfile(os.path.join(init, f)):
+                shutil.copyfile(os.path.join(init, f),
+                                os.path.join(out_dir, f))
     return train(teacher_dir, out_dir, frames, elem, labels, epochs, batch,
                  lr, w_energy, w_force, device=device, log=log,
-                 lr_final=lr_final)
+                 lr_final=lr_final, decay_epochs=decay_epochs)
 
 
 def main():
@@ -227,13 +243,22 @@ def main():
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--lr-final", type=float, default=None,
                    help="decay the learning rate linearly to this value "
-                        "over the last five epochs")
+                        "over the last --decay-epochs epochs")
+    t.add_argument("--decay-epochs", type=int, default=5)
     t.add_argument("--w-energy", type=float, default=1.0)
     t.add_argument("--w-force", type=float, default=1.0)
+    t.add_argument("--sigma", type=float, default=0.15,
+                   help="position noise of the training frames (bohr)")
+    t.add_argument("--sigma-max", type=float, default=None,
+                   help="draw the noise per frame from U[sigma, sigma-max]")
+    t.add_argument("--init", default=None,
+                   help="continue training this student directory")
     args = a.parse_args()
     r = distill(args.teacher, args.out, args.frames, args.epochs, args.batch,
                 args.lr, args.hidden, args.seed, lr_final=args.lr_final,
-                w_energy=args.w_energy, w_force=args.w_force)
+                w_energy=args.w_energy, w_force=args.w_force,
+                decay_epochs=args.decay_epochs, init=args.init,
+                sigma=args.sigma, sigma_max=args.sigma_max)
     print(f"trained: {r['steps']} steps in {r['seconds']:.0f} s")
 
 
