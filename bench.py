@@ -352,7 +352,7 @@ def _stage_ms(p, frames_dev, steps):
 def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
     """Plain FP64 vs the mixed forms on the same 24,576-atom frames, for the
     52-SF potential and the wider 92-SF / 64-64-64 softplus potential, and
-    for the latter the distilled 92-16-1 student (gated by its training
+    for the latter the distilled 92-32-1 student (gated by its training
     range; atoms outside it are re-evaluated by the teacher on the tensor
     cores).  Accuracy is measured against the FP64 form on three frames (the
     FP64 form equals the reference to 1e-10, tests/test_gpu_parity.py) and,
@@ -430,7 +430,7 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
                  "hi/lo operand pairs (3 MMAs per step), FP32 accumulation; "
                  "FP64 displacements, energy sum, force accumulation",
         "bf16": "as mixed with single BF16 operands (1 MMA per step)",
-        "student_gated": "FP32 symmetry functions; distilled 92-16-1 FP32 "
+        "student_gated": "FP32 symmetry functions; distilled 92-32-1 FP32 "
                          "student for atoms inside its training range, the "
                          "mixed-precision teacher for the others",
         "student_only": "the student for every atom (no gate)"}

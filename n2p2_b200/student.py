@@ -1,7 +1,7 @@
 """Distillation of a small student atomic network from an n2p2 potential.
 
     python -m n2p2_b200.student train --teacher DIR --out DIR \
-        [--frames 500] [--epochs 20] [--batch 4096] [--lr 1e-3] [--hidden 16]
+        [--frames 500] [--epochs 20] [--batch 4096] [--lr 1e-3] [--hidden 32]
         [--lr-final LR] [--decay-epochs 5] [--w-energy 1] [--w-force 1]
         [--sigma-max S] [--init STUDENT_DIR]
 
@@ -199,7 +199,7 @@ def train(teacher_dir: str, student_dir: str, frames, elem, labels,
 
 
 def distill(teacher_dir: str, out_dir: str, n_frames=500, epochs=20,
-            batch=4096, lr=1e-3, hidden=16, seed=0, device=0, log=print,
+            batch=4096, lr=1e-3, hidden=32, seed=0, device=0, log=print,
             lr_final=None, w_energy=1.0, w_force=1.0, decay_epochs=5,
             init=None, sigma=0.15, sigma_max=None):
     """Labels the training frames with the teacher and trains a student in
@@ -239,7 +239,7 @@ def main():
     t.add_argument("--epochs", type=int, default=20)
     t.add_argument("--batch", type=int, default=4096)
     t.add_argument("--lr", type=float, default=1e-3)
-    t.add_argument("--hidden", type=int, default=16)
+    t.add_argument("--hidden", type=int, default=32)
     t.add_argument("--seed", type=int, default=0)
     t.add_argument("--lr-final", type=float, default=None,
                    help="decay the learning rate linearly to this value "
