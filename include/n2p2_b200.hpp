@@ -243,10 +243,97 @@ public:
     void setPrecision(int mode) { check(ctx_, n2p2b_set_precision(ctx_,
                                                                   mode)); }
 
+    // Mode::initialize (libnnp/Mode.cpp:55) only writes the reference's
+    // banner to its log; a context needs no such step.
+    void initialize() {}
+    // Mode::setupSymmetryFunctionGroups: setupGeneric builds the groups (as
+    // the reference's setupGeneric does, libnnp/Mode.cpp:231), so a call
+    // after it has nothing left to do.
+    void setupSymmetryFunctionGroups() {}
+
     // Mode::evaluateNNP on a structure (its element indices are resolved
     // from the symbols), followed by Prediction::predict's unit conversion
     // and offsets; fills energy, f and atomEnergy.
     void evaluate(Structure& s, bool remap = true)
+    {
+        upload(s, remap);
+        check(ctx_, n2p2b_evaluate(ctx_, 1));
+        fetchAtomicEnergies(s);
+        fetchEnergy(s);
+        fetchForces(s);
+    }
+
+    // The evaluation steps of nnp::Mode (libnnp/Mode.h) on a structure.  The
+    // reference's callers build the neighbor list first
+    // (Structure::calculateNeighborList); calculateSymmetryFunctionGroups
+    // uploads the structure and builds it.  Each step leaves its result in
+    // the structure in the units Prediction::predict leaves there (physical
+    // units; the energy with the atoms' offset energies).
+    void calculateSymmetryFunctionGroups(Structure& s, bool derivatives,
+                                         bool remap = true)
+    {
+        upload(s, remap);
+        check(ctx_, n2p2b_calculate_neighbor_list(ctx_));
+        check(ctx_, n2p2b_calculate_symmetry_function_groups(ctx_,
+                                                             derivatives));
+    }
+    // Mode::calculateAtomicNeuralNetworks; id selects the network of a
+    // 4G potential in the reference, and a 2G potential has only "short".
+    void calculateAtomicNeuralNetworks(Structure& s, bool derivatives,
+                                       std::string const& id = "")
+    {
+        if (!id.empty() && id != "short")
+            throw std::invalid_argument("ERROR: Only the short-range network "
+                                        "(2G) is available.\n");
+        check(ctx_, n2p2b_calculate_atomic_neural_networks(ctx_,
+                                                           derivatives));
+        fetchAtomicEnergies(s);
+    }
+    void calculateEnergy(Structure& s) const
+    {
+        check(ctx_, n2p2b_calculate_energy(ctx_));
+        fetchEnergy(s);
+    }
+    void calculateForces(Structure& s) const
+    {
+        check(ctx_, n2p2b_calculate_forces(ctx_));
+        fetchForces(s);
+    }
+    // Mode::evaluateNNP (libnnp/Mode.cpp:1967-2016): neighbor list,
+    // symmetry functions (derivatives with forces), networks (derivatives
+    // with forces or dE/dG), energy, forces.
+    void evaluateNNP(Structure& s, bool useForces = true, bool useDEdG = true,
+                     bool remap = true)
+    {
+        useDEdG = useForces || useDEdG;
+        if (useDEdG && !useForces)
+        {
+            calculateSymmetryFunctionGroups(s, false, remap);
+            calculateAtomicNeuralNetworks(s, true);
+            calculateEnergy(s);
+            return;
+        }
+        upload(s, remap);
+        check(ctx_, n2p2b_evaluate(ctx_, useForces ? 1 : 0));
+        fetchAtomicEnergies(s);
+        fetchEnergy(s);
+        if (useForces) fetchForces(s);
+    }
+
+    // Mode::getEnergyOffset: sum of the atoms' offset energies.
+    double getEnergyOffset(Structure const& s) const
+    {
+        double e = 0.0;
+        for (int32_t el : s.element) e += atomicEnergyOffset(el);
+        return e;
+    }
+
+protected:
+    n2p2b_context* ctx_ = nullptr;
+
+    // Uploads a structure: element indices from the symbols, positions and
+    // box (wrapped into the cell with remap, as Structure::remap).
+    void upload(Structure& s, bool remap)
     {
         std::size_t const n = s.numAtoms();
         s.element.resize(n);
@@ -263,24 +350,21 @@ public:
                                         s.r.data(), N2P2B_HOST,
                                         s.element.data(),
                                         remap ? N2P2B_REMAP : 0));
-        check(ctx_, n2p2b_evaluate(ctx_, 1));
-        s.f.resize(3 * n);
-        s.atomEnergy.resize(n);
-        check(ctx_, n2p2b_get_energy(ctx_, &s.energy));
-        check(ctx_, n2p2b_get_forces(ctx_, s.f.data(), N2P2B_HOST));
+    }
+    void fetchAtomicEnergies(Structure& s) const
+    {
+        s.atomEnergy.resize(s.numAtoms());
         check(ctx_, n2p2b_get_atomic_energies(ctx_, s.atomEnergy.data()));
     }
-
-    // Mode::getEnergyOffset: sum of the atoms' offset energies.
-    double getEnergyOffset(Structure const& s) const
+    void fetchEnergy(Structure& s) const
     {
-        double e = 0.0;
-        for (int32_t el : s.element) e += atomicEnergyOffset(el);
-        return e;
+        check(ctx_, n2p2b_get_energy(ctx_, &s.energy));
     }
-
-protected:
-    n2p2b_context* ctx_ = nullptr;
+    void fetchForces(Structure& s) const
+    {
+        s.f.resize(3 * s.numAtoms());
+        check(ctx_, n2p2b_get_forces(ctx_, s.f.data(), N2P2B_HOST));
+    }
 };
 
 class Prediction : public Mode

@@ -50,3 +50,45 @@ def test_null_context_is_rejected():
     L = _capi.load()
     assert L.n2p2b_evaluate(None, 1) == _capi.ERR_ARGUMENT
     assert L.n2p2b_last_error(None) == b"null context"
+
+
+def test_cpp_wrapper_mirrors_mode_api(tmp_path):
+    """The C++ header (nnp::Mode / Prediction / InterfaceLammps names over
+    the C ABI) compiles and links a caller that uses the reference's
+    evaluation steps (libnnp/Mode.h) and Prediction flow; nothing runs."""
+    import shutil
+    import subprocess
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.cpp"
+    src.write_text(r'''
+#include "n2p2_b200.hpp"
+int main(int argc, char** argv)
+{
+    if (argc < 2) return 0;
+    n2p2b::Prediction p(0);
+    p.initialize();
+    p.setup();
+    p.setupSymmetryFunctionGroups();
+    p.readStructureFromFile(argv[1]);
+    n2p2b::Structure& s = p.structure;
+    p.calculateSymmetryFunctionGroups(s, true);
+    p.calculateAtomicNeuralNetworks(s, true);
+    p.calculateEnergy(s);
+    p.calculateForces(s);
+    p.evaluateNNP(s);
+    p.evaluateNNP(s, false, true);
+    p.predict();
+    return p.getMaxCutoffRadius() > 0.0 ? 0 : 1;
+}
+''')
+    lib = os.path.join(root, "n2p2_b200")
+    if not os.path.exists(os.path.join(lib, "libn2p2b200.so")):
+        pytest.skip("library not built")
+    r = subprocess.run([gxx, "-std=c++17", "-I" + os.path.join(root, "include"),
+                        str(src), "-o", str(tmp_path / "caller"),
+                        "-L" + lib, "-ln2p2b200"],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
