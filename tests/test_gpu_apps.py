@@ -110,3 +110,92 @@ def test_interface_lammps_emulation(gpu, tmp_path, cf):
     e0, f0 = _reference(box, pos, elem)
     # Engine units: E / cfenergy, F * cflength / cfenergy.
     _check(e * cfe, f * cfe / cfl, e0, f0)
+
+
+_STEPS_CALLER = r'''
+#include <cstdio>
+#include "n2p2_b200.hpp"
+
+static void dump(std::FILE* o, char const* tag, n2p2b::Structure const& s,
+                 bool forces)
+{
+    std::fprintf(o, "%s %.17g\n", tag, s.energy);
+    if (forces)
+        for (double v : s.f) std::fprintf(o, "%.17g\n", v);
+}
+
+int main()
+{
+    n2p2b::Prediction p(0);
+    p.initialize();
+    p.setup();
+    p.setupSymmetryFunctionGroups();
+    p.readStructureFromFile("input.data");
+    std::FILE* o = std::fopen("steps.out", "w");
+    n2p2b::Structure s = p.structure;
+    p.calculateSymmetryFunctionGroups(s, true);
+    p.calculateAtomicNeuralNetworks(s, true);
+    p.calculateEnergy(s);
+    p.calculateForces(s);
+    dump(o, "steps", s, true);
+    n2p2b::Structure s2 = p.structure;
+    p.evaluateNNP(s2);
+    dump(o, "evaluateNNP", s2, true);
+    n2p2b::Structure s3 = p.structure;
+    p.evaluateNNP(s3, false, true);
+    dump(o, "energy_dEdG", s3, false);
+    n2p2b::Structure s4 = p.structure;
+    p.evaluateNNP(s4, false, false);
+    dump(o, "energy_only", s4, false);
+    p.predict();
+    dump(o, "predict", p.structure, true);
+    std::fclose(o);
+    return 0;
+}
+'''
+
+
+def test_cpp_mode_steps_match_reference(gpu, tmp_path):
+    """n2p2b::Prediction driven through the nnp::Mode evaluation steps
+    (calculateSymmetryFunctionGroups -> calculateAtomicNeuralNetworks ->
+    calculateEnergy -> calculateForces), evaluateNNP with and without forces
+    and predict(): all equal to the reference library (energy 1e-10
+    relative, forces 1e-10 of max(|F|, rms F)); the energy-only forms
+    within 1e-12 of evaluateNNP's energy."""
+    gxx = shutil.which("g++")
+    if gxx is None:
+        pytest.skip("g++ not available")
+    lib = os.path.join(ROOT, "n2p2_b200")
+    src = tmp_path / "steps.cpp"
+    src.write_text(_STEPS_CALLER)
+    exe = tmp_path / "steps"
+    r = subprocess.run([gxx, "-std=c++17", "-O2",
+                        "-I" + os.path.join(ROOT, "include"), str(src),
+                        "-L" + lib, "-ln2p2b200", "-Wl,-rpath," + lib,
+                        "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    box, pos, elem = synth.water_box(64, 33)
+    pos = pos + np.random.default_rng(6).normal(0, 0.1, pos.shape)
+    for name in ("input.nn", "scaling.data", "weights.001.data",
+                 "weights.008.data"):
+        shutil.copy(os.path.join(POT, name), tmp_path / name)
+    _write_input_data(tmp_path / "input.data", box, pos, elem)
+    r = subprocess.run([str(exe)], cwd=tmp_path, capture_output=True,
+                       text=True)
+    assert r.returncode == 0, r.stderr
+    blocks, cur = {}, None
+    for ln in open(tmp_path / "steps.out"):
+        t = ln.split()
+        if len(t) == 2:
+            cur = t[0]
+            blocks[cur] = [float(t[1]), []]
+        else:
+            blocks[cur][1].append(float(t[0]))
+    n = len(elem)
+    e0, f0 = _reference(box, pos, elem)
+    for tag in ("steps", "evaluateNNP", "predict"):
+        e, f = blocks[tag][0], np.array(blocks[tag][1]).reshape(n, 3)
+        _check(e, f, e0, f0)
+    e1 = blocks["evaluateNNP"][0]
+    for tag in ("energy_dEdG", "energy_only"):
+        assert abs(blocks[tag][0] - e1) <= 1e-12 * abs(e1)
