@@ -506,8 +506,12 @@ class Mode:
                                         collectExtrapolationWarnings,
                                         writeExtrapolationWarnings,
                                         stopOnExtrapolationWarnings):
+        """Extrapolation warnings as the reference counts, writes and stops
+        on them.  collectStatistics (per-SF statistics for the training
+        tools, which pynnp offers no way to read) is accepted and not
+        collected."""
         self._m.setup_symmetry_function_statistics(
-            collectStatistics, collectExtrapolationWarnings,
+            False, collectExtrapolationWarnings,
             writeExtrapolationWarnings, stopOnExtrapolationWarnings)
 
     # ---- queries -----------------------------------------------------------

@@ -122,7 +122,7 @@ def test_mode_step_example_with_normalization(gpu, tmp_path):
     m.setupNeuralNetwork()
     m.setupSymmetryFunctionScaling(os.path.join(d, "scaling.data"))
     m.setupNeuralNetworkWeights(os.path.join(d, "weights.%03zu.data"))
-    m.setupSymmetryFunctionStatistics(False, False, False, False)
+    m.setupSymmetryFunctionStatistics(True, True, True, False)
     s = pynnp.Structure()
     s.setElementMap(m.elementMap)
     s.readFromFile(os.path.join(d, "input.data"))

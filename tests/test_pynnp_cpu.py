@@ -45,7 +45,7 @@ def _host_mode():
     m.setupNeuralNetwork()
     m.setupSymmetryFunctionScaling(os.path.join(POT, "scaling.data"))
     m.setupNeuralNetworkWeights(os.path.join(POT, "weights.%03zu.data"))
-    m.setupSymmetryFunctionStatistics(False, False, False, False)
+    m.setupSymmetryFunctionStatistics(True, True, True, False)
     return m
 
 
