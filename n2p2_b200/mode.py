@@ -135,6 +135,18 @@ class Mode:
     def get_max_cutoff_radius(self) -> float:
         return self._L.n2p2b_max_cutoff_radius(self._h)
 
+    def unit_conversion(self):
+        """(normalizes, mean_energy, conv_energy, conv_length) of input.nn
+        (0, 1, 1 without normalization)."""
+        mean, ce, cl = C.c_double(), C.c_double(), C.c_double()
+        flag = self._L.n2p2b_unit_conversion(self._h, C.byref(mean),
+                                             C.byref(ce), C.byref(cl))
+        return bool(flag == 1), mean.value, ce.value, cl.value
+
+    def atomic_energy_offset(self, e: int) -> float:
+        """Element::getAtomicEnergyOffset (atom_energy of input.nn)."""
+        return self._L.n2p2b_atomic_energy_offset(self._h, e)
+
     def symmetry_function_params(self, e: int, s: int):
         """type, e1, e2, eta, rs, rc, zeta, lambda, scaling factor, line
         (Element::getSymmetryFunction(s), normalized units)."""

@@ -523,11 +523,7 @@ class Mode:
         return self._m.get_max_cutoff_radius()
 
     def _units(self):
-        import ctypes as C
-        mean, ce, cl = C.c_double(), C.c_double(), C.c_double()
-        flag = self._m._L.n2p2b_unit_conversion(self._m._h, C.byref(mean),
-                                                C.byref(ce), C.byref(cl))
-        return bool(flag == 1), mean.value, ce.value, cl.value
+        return self._m.unit_conversion()
 
     def useNormalization(self):
         return self._units()[0]
@@ -563,7 +559,7 @@ class Mode:
 
     # ---- energy offsets ----------------------------------------------------
     def _offset(self, s):
-        return sum(c * self._m._L.n2p2b_atomic_energy_offset(self._m._h, e)
+        return sum(c * self._m.atomic_energy_offset(e)
                    for e, c in enumerate(s.numAtomsPerElement))
 
     def addEnergyOffset(self, structure, ref=True):
