@@ -429,7 +429,7 @@ public:
         setupSymmetryFunctionScaling(dir + "scaling.data");
         setupSymmetryFunctionStatistics(false, showew || showewsum > 0
                                                    || maxew >= 0,
-                                        false, false);
+                                        showew, false);
         setupNeuralNetworkWeights(dir + "weights.%03zu.data");
         if (lammpsCutoff < getMaxCutoffRadiusLammps())
             throw std::runtime_error("ERROR: LAMMPS cutoff via pair_coeff "
@@ -576,6 +576,28 @@ public:
             for (int c = 0; c < 3; ++c)
                 atomF[m][c] += forces_[3 * (std::size_t)m + c] * cf;
     }
+    // Extrapolation-warning output (InterfaceLammps.cpp:638-776).  With
+    // showew the library writes the reference's warning lines
+    // (Element.cpp:505-518) while process() runs, so
+    // writeExtrapolationWarnings has nothing left to write.  The reference's
+    // EW buffers carry per-SF statistics records from the other MPI ranks
+    // to rank 0; here every rank writes its own lines, so no records travel
+    // and the buffer is empty (as in the reference built without MPI).
+    long getEWBufferSize() const { return 0; }
+    void fillEWBuffer(char* const& buf, int bs) const
+    {
+        (void)buf;
+        (void)bs;
+    }
+    void extractEWBuffer(char const* const& buf, int bs)
+    {
+        (void)buf;
+        (void)bs;
+    }
+    void writeExtrapolationWarnings() {}
+    // SymFncStatistics::clear on every element: the warnings and their count.
+    void clearExtrapolationWarnings() { resetExtrapolationWarnings(); }
+
     // In LAMMPS units.
     double getMaxCutoffRadiusLammps() const
     {

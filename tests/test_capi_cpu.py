@@ -81,6 +81,14 @@ int main(int argc, char** argv)
     p.evaluateNNP(s);
     p.evaluateNNP(s, false, true);
     p.predict();
+    n2p2b::InterfaceLammps lmp(0);
+    lmp.initialize(".", "", true, false, 0, -1, 1.0, 1.0, 12.0, 2, 0);
+    char* buf = new char[lmp.getEWBufferSize() + 1];
+    lmp.fillEWBuffer(buf, (int)lmp.getEWBufferSize());
+    lmp.extractEWBuffer(buf, (int)lmp.getEWBufferSize());
+    lmp.writeExtrapolationWarnings();
+    lmp.clearExtrapolationWarnings();
+    delete[] buf;
     return p.getMaxCutoffRadius() > 0.0 ? 0 : 1;
 }
 ''')
