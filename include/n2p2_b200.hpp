@@ -199,6 +199,15 @@ public:
         check(ctx_, n2p2b_setup_neural_network_weights(ctx_,
                                                         format.c_str()));
     }
+    // The reference's form with one file-name format per network type
+    // (libnnp/Mode.h): a 2G potential reads the "short" networks only.
+    void setupNeuralNetworkWeights(
+        std::map<std::string, std::string> const& formats)
+    {
+        auto const it = formats.find("short");
+        setupNeuralNetworkWeights(it != formats.end() ? it->second
+                                                      : "weights.%03zu.data");
+    }
     void setupSymmetryFunctionStatistics(bool collectStatistics,
                                          bool collectExtrapolationWarnings,
                                          bool writeExtrapolationWarnings,
@@ -375,6 +384,7 @@ public:
     std::string fileNameSettings = "input.nn";
     std::string fileNameScaling = "scaling.data";
     std::string formatWeightsFilesShort = "weights.%03zu.data";
+    std::string formatWeightsFilesCharge = "weightse.%03zu.data"; // 4G only
     Structure   structure;
 
     // Prediction::setup (libnnp/Prediction.cpp:34-46).

@@ -72,6 +72,11 @@ int main(int argc, char** argv)
     p.initialize();
     p.setup();
     p.setupSymmetryFunctionGroups();
+    std::map<std::string, std::string> formats{
+        {"short", p.formatWeightsFilesShort},
+        {"elec", p.formatWeightsFilesCharge}};
+    p.setupNeuralNetworkWeights(formats);
+    p.setupNeuralNetworkWeights("weights.%03zu.data");
     p.readStructureFromFile(argv[1]);
     n2p2b::Structure& s = p.structure;
     p.calculateSymmetryFunctionGroups(s, true);
