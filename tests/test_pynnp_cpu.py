@@ -148,3 +148,48 @@ def test_prediction_host_setup_and_read(tmp_path):
         p.close()
     finally:
         os.chdir(cwd)
+
+
+def test_structure_parser_edge_cases():
+    """begin arguments, comment text, open (non-periodic) structures, a
+    triclinic cell and the reference's errors for malformed input."""
+    em = pynnp.ElementMap(["H", "O"])
+    s = pynnp.Structure()
+    s.setElementMap(em)
+    s.readFromLines(["begin set=train", "comment  two  words ",
+                     "atom 0 0 0 O 0.5 0 1 2 3",
+                     "atom 1 0 0 H -0.25 0 0 0 0",
+                     "energy -1.5", "charge 0.25", "end"])
+    assert s.sampleType == 1 and not s.isPeriodic
+    assert s.comment == " two  words "
+    assert s.numAtomsPerElement == [1, 1] and s.chargeRef == 0.25
+    assert [a.chargeRef for a in s.atoms] == [0.5, -0.25]
+    assert s.atoms[0].fRef.r == [1.0, 2.0, 3.0]
+    t = pynnp.Structure()
+    t.setElementMap(em)
+    t.readFromLines(["begin", "lattice 10 0 0", "lattice 1 10 0",
+                     "lattice 0 0 10", "atom 0 0 0 H 0 0 0 0 0", "end"])
+    assert t.isPeriodic and t.isTriclinic and np.isclose(t.volume, 1000.0)
+    for bad in (["atom 0 0 0 H 0 0 0 0 0", "end"],
+                ["begin set=other", "end"],
+                ["begin", "lattice 1 0 0", "end"],
+                ["begin", "velocity 0 0 0", "end"]):
+        u = pynnp.Structure()
+        u.setElementMap(em)
+        with pytest.raises(RuntimeError):
+            u.readFromLines(bad)
+
+
+def test_mode_steps_need_symmetry_functions_first():
+    m = _host_mode()
+    s = pynnp.Structure()
+    s.setElementMap(m.elementMap)
+    s.readFromLines(["begin", "atom 0 0 0 H 0 0 0 0 0", "end"])
+    with pytest.raises(RuntimeError):
+        m.calculateAtomicNeuralNetworks(s, True)
+    with pytest.raises(RuntimeError):
+        m.calculateSymmetryFunctionGroups(s, True)   # no neighbor list yet
+    s.calculateNeighborList(1.0)
+    with pytest.raises(ValueError):
+        m.calculateSymmetryFunctionGroups(s, True)   # cutoff below 12
+    m.close()
