@@ -507,16 +507,11 @@ def measure_batch(stream, lib, local, n_structures=4096, steps=5):
 
 def run_ours(a):
     import torch
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(
-            seconds=600), device_id=torch.device("cuda", local))
+    from n2p2_b200.replicas import Replicas
+    # One process per GPU, each on its own frames (weak scaling); NCCL only
+    # for the barrier and the maximum of the ranks' times.
+    rep = Replicas("nccl")
+    world, rank, local = rep.world, rep.rank, rep.local
 
     from n2p2_b200 import _capi
     from n2p2_b200.mode import Prediction
@@ -542,18 +537,6 @@ def run_ours(a):
     tune = p.autotune(True, 1)
     lib = _capi.load()
 
-    def barrier():
-        torch.cuda.synchronize()
-        if dist is not None:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
     # ---- warm-up ---------------------------------------------------------
     for s in range(max(a.warmup, 3)):
         p.set_positions(dev_frames[s % F])
@@ -562,13 +545,13 @@ def run_ours(a):
 
     with ClockSampler(local) as clocks:
         # ---- value: device-resident frames -------------------------------
-        barrier()
+        rep.barrier()
         t_dev, launches = _time_steps(p, dev_frames, a.steps, stream, lib)
-        barrier()
-        t_dev = max_over_ranks(t_dev)
+        rep.barrier()
+        t_dev = rep.max(t_dev)
 
         # ---- e2e: host buffers through the C-ABI -------------------------
-        barrier()
+        rep.barrier()
         t0 = time.perf_counter()
         energy = 0.0
         for s in range(a.steps):
@@ -577,8 +560,8 @@ def run_ours(a):
             p._check(lib.n2p2b_get_forces(p._h, host_forces.data_ptr(),
                                           _capi.HOST))
             energy = p.energy
-        barrier()
-        t_e2e = max_over_ranks(time.perf_counter() - t0)
+        rep.barrier()
+        t_e2e = rep.max(time.perf_counter() - t0)
 
         # ---- profiled pass: per-stage device time -------------------------
         per = _stage_ms(p, dev_frames, a.steps)
@@ -592,15 +575,13 @@ def run_ours(a):
         if world == 1 and not a.no_batch:
             batch = measure_batch(stream, lib, local)
 
-    if dist is not None:
-        dist.barrier()
+    rep.barrier()
 
     atoms_total = n * a.steps * world
     value = atoms_total / t_dev
     e2e = atoms_total / t_e2e
     if rank != 0:
-        if dist is not None:
-            dist.destroy_process_group()
+        rep.close()
         return
 
     # ---- roofline of the dominant kernel (symmetry functions) -------------
@@ -652,8 +633,7 @@ def run_ours(a):
     if not a.no_cpu_baseline and world == 1:
         line["cpu_baseline"] = cpu_baseline(frames, box, elem)
     print(json.dumps(line))
-    if dist is not None:
-        dist.destroy_process_group()
+    rep.close()
 
 
 def main():
