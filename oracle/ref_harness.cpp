@@ -149,6 +149,13 @@ void* refh_create(char const* dir, int unscaled)
         h->unscaled = (unscaled != 0);
         if (h->unscaled) h->model.setupUnscaled();
         else             h->model.setup();
+        // The reference logs its low-neighbor-count warning from inside the
+        // OpenMP loop over atoms (Mode::calculateSymmetryFunctionGroups,
+        // libnnp/Mode.cpp:1598-1609), and Log::addLogEntry appends to a
+        // shared std::vector (libnnp/Log.cpp): several threads warning at
+        // once (a small open molecule, e.g. DMABN_SCAN) corrupt the heap.
+        // A silent log stores nothing; the numbers are unaffected.
+        h->model.log.silent = true;
     }
     catch (exception const& e)
     {

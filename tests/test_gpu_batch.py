@@ -39,8 +39,13 @@ def _noisy(structs, seed):
 
 
 def _check_against_reference(p, structs):
+    """Per structure: neighbor list bit-exact, energy 1e-10 relative, forces
+    1e-10 max(|F|, rms F).  Returns the largest relative energy and force
+    errors over the structures."""
     from oracle.ref import RefModel
     ref = RefModel(POT)
+    ref.setup_statistics()
+    worst_e = worst_f = 0.0
     E = p.structure_energies()
     F = p.forces()
     cnt, idx, dr, d = p.neighbor_list()
@@ -60,10 +65,13 @@ def _check_against_reference(p, structs):
         er, fr = ref.predict()
         assert abs(E[s] - er) <= 1e-10 * abs(er)
         f = F[a0:a0 + n]
-        tol = 1e-10 * np.maximum(np.abs(fr), np.sqrt(np.mean(fr ** 2)))
-        assert np.all(np.abs(f - fr) <= tol)
+        scale = np.maximum(np.abs(fr), np.sqrt(np.mean(fr ** 2)))
+        assert np.all(np.abs(f - fr) <= 1e-10 * scale)
+        worst_e = max(worst_e, abs(E[s] - er) / abs(er))
+        worst_f = max(worst_f, float((np.abs(f - fr) / scale).max()))
         a0 += n
         e0 += m
+    return worst_e, worst_f
 
 
 def test_batch_matches_reference_per_structure(gpu):
@@ -74,6 +82,24 @@ def test_batch_matches_reference_per_structure(gpu):
     _check_against_reference(p, structs)
     assert abs(p.energy - p.structure_energies().sum()) <= 1e-12 * abs(
         p.energy)
+
+
+def test_batch_full_size_range(gpu):
+    """The batching workload's whole size range, 11-171 molecules (33-513
+    atoms): 38 structures drawn from it plus one of each extreme size, in
+    one batch, each against the reference alone."""
+    structs = synth.batch_structures(38, 2029, lo=11, hi=171)
+    for nmol, seed in ((11, 71), (171, 72)):
+        structs.append(synth.water_box(nmol, seed))
+    structs = _noisy(structs, 3)
+    sizes = [len(s[2]) for s in structs]
+    assert min(sizes) == 33 and max(sizes) == 513
+    p = _pred()
+    p.set_structures(structs)
+    p.evaluate_nnp(True)
+    we, wf = _check_against_reference(p, structs)
+    print(f"{len(structs)} structures of {min(sizes)}-{max(sizes)} atoms: "
+          f"max relative energy error {we:.1e}, force {wf:.1e}")
 
 
 def test_graph_replay_equals_direct_evaluation(gpu):

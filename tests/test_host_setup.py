@@ -11,7 +11,7 @@ import os
 import numpy as np
 import pytest
 
-from conftest import REFERENCE, reference_tree_available
+from conftest import REF_EXAMPLES
 from oracle import ref as oref
 
 POT = os.path.join(os.path.dirname(__file__), "golden", "potentials")
@@ -23,11 +23,9 @@ needs_ref_lib = pytest.mark.skipif(not oref.ref_available(),
 def potential_dirs():
     out = [os.path.join(POT, d) for d in sorted(os.listdir(POT))
            if os.path.exists(os.path.join(POT, d, "input.nn"))]
-    if reference_tree_available():
-        for name in ("H2O_RPBE-D3", "Cu2S_PBE", "Ethylbenzene_SCAN",
-                     "DMABN_SCAN", "Anisole_SCAN"):
-            out.append(os.path.join(REFERENCE, "examples", "nnp-predict",
-                                    name))
+    for name in ("H2O_RPBE-D3", "Cu2S_PBE", "Ethylbenzene_SCAN",
+                 "DMABN_SCAN", "Anisole_SCAN"):
+        out.append(os.path.join(REF_EXAMPLES, name))
     return out
 
 

@@ -2,9 +2,10 @@
 
 * The reference library built from the reference sources (oracle/_ref) and
   the C restatement (oracle/hdnnp_oracle.c) both reproduce the reference's
-  own golden energies and forces of test/cpp/ExamplePrediction.h -- read from
-  the reference tree at test time, never copied -- within the reference's
-  tolerance 1000 * DBL_EPSILON (test/cpp/test_Prediction.cpp:27).
+  own golden energies and forces of test/cpp/ExamplePrediction.h (committed
+  with the example inputs under tests/golden/ref_examples by
+  make_ref_examples.py) within the reference's tolerance 1000 * DBL_EPSILON
+  (test/cpp/test_Prediction.cpp:27).
 * The restatement agrees with the reference library on the synthetic water
   potentials (neighbor lists exactly, energies/forces to 1e-12 relative).
 """
@@ -13,53 +14,47 @@ import os
 import numpy as np
 import pytest
 
-from conftest import REFERENCE, reference_tree_available
+from conftest import REF_EXAMPLES, ref_example
 from oracle import ref as oref
 from oracle import restated
 
 POT = os.path.join(os.path.dirname(__file__), "golden", "potentials")
 EPS1000 = 1000.0 * np.finfo(float).eps
+# The restatement covers SF types 2, 3 and 9; the compact types of the
+# other three examples are pinned against the reference build only.
 EXAMPLES = ["H2O_RPBE-D3", "Cu2S_PBE"]
+ALL_EXAMPLES = ["H2O_RPBE-D3", "Cu2S_PBE", "Ethylbenzene_SCAN",
+                "Anisole_SCAN", "DMABN_SCAN"]
 
-needs_ref_tree = pytest.mark.skipif(
-    not reference_tree_available(), reason="reference tree not present")
 needs_ref_lib = pytest.mark.skipif(
     not oref.ref_available(), reason="oracle/_ref not built")
 
 
 def _example(name):
-    d = os.path.join(REFERENCE, "examples", "nnp-predict", name)
-    fr = oref.read_input_data(os.path.join(d, "input.data"))[0]
-    syms = restated.Potential(d).symbols
-    elem = np.array([syms.index(s) for s in fr["sym"]], dtype=np.int32)
-    return d, fr, elem
+    from n2p2_b200.mode import Prediction
+    d, box, pos, sym, ge, gf = ref_example(name)
+    host = Prediction(d, device=-1)       # host-only: element order
+    host.setup()
+    elem = host.element_indices(sym)
+    host.close()
+    return d, box, pos, elem, ge, gf
 
 
-@pytest.fixture(scope="module")
-def golden():
-    return oref.read_golden_prediction(os.path.join(
-        REFERENCE, "test", "cpp", "ExamplePrediction.h"))
-
-
-@needs_ref_tree
 @needs_ref_lib
-@pytest.mark.parametrize("name", EXAMPLES)
-def test_reference_build_matches_golden(golden, name):
-    d, fr, elem = _example(name)
+@pytest.mark.parametrize("name", ALL_EXAMPLES)
+def test_reference_build_matches_golden(name):
+    d, box, pos, elem, ge, gf = _example(name)
     m = oref.RefModel(d)
-    m.set_structure(fr["pos"], elem, fr["box"])
+    m.set_structure(pos, elem, box)
     e, f = m.predict()
-    ge, gf = golden[name]
     assert abs(e - ge) <= EPS1000 * max(1.0, abs(ge)) or abs(e - ge) <= EPS1000
     assert np.abs(f - gf).max() <= EPS1000
 
 
-@needs_ref_tree
 @pytest.mark.parametrize("name", EXAMPLES)
-def test_restatement_matches_golden(golden, name):
-    d, fr, elem = _example(name)
-    e, f = restated.predict(d, fr["pos"], elem, fr["box"])
-    ge, gf = golden[name]
+def test_restatement_matches_golden(name):
+    d, box, pos, elem, ge, gf = _example(name)
+    e, f = restated.predict(d, pos, elem, box)
     assert abs(e - ge) <= EPS1000 * max(1.0, abs(ge))
     assert np.abs(f - gf).max() <= EPS1000
 
@@ -105,24 +100,17 @@ def test_restated_neighbor_list_is_the_reference_list():
 
 
 def cutoff_kats():
-    """(rc, alpha, r, f[9], df[9]) of test/cpp/test_CutoffFunction.cpp."""
-    import re
-    src = open(os.path.join(REFERENCE, "test", "cpp",
-                            "test_CutoffFunction.cpp")).read()
-    rc = float(re.search(r"cutoffRadius\s*=\s*([0-9.eE+-]+);", src).group(1))
-    alpha = float(re.search(r"cutoffParameter\s*=\s*([0-9.eE+-]+);",
-                            src).group(1))
-    frac = float(re.search(r"testRadius\s*=\s*([0-9.eE+-]+)\s*\*", src)
-                 .group(1))
-
-    def vec(name):
-        body = re.search(r"vector<double> const " + name + r"\s*=\s*\{(.*?)\}",
-                         src, re.S).group(1)
-        return [float(x) for x in body.replace("\n", " ").split(",")]
-    return rc, alpha, frac * rc, vec("f"), vec("df")
+    """(rc, alpha, r, f[9], df[9]): the known answers of the reference's
+    test/cpp/test_CutoffFunction.cpp (tests/golden/ref_examples/
+    cutoff_kats.txt, written by make_ref_examples.py)."""
+    with open(os.path.join(REF_EXAMPLES, "cutoff_kats.txt")) as fh:
+        w = fh.readline().split()
+        rc, alpha, r = float(w[1]), float(w[3]), float(w[5])
+        rows = [ln.split() for ln in fh if ln.strip()]
+    return (rc, alpha, r, [float(x[1]) for x in rows],
+            [float(x[2]) for x in rows])
 
 
-@needs_ref_tree
 def test_cutoff_kats_all_types():
     """All nine cutoff types at r = 0.8 rc (rc = 3, alpha = 0.2) against the
     reference's known answers, tolerance 100 * DBL_EPSILON as there."""
