@@ -1,6 +1,9 @@
 """Energy + force throughput of the n2p2 prediction path on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py --profile-case [--molecules M] [--potential P]
+                    [--precision fp64|mixed|bf16] [--evaluations E]
+                    [--autotune]
 
 Workload (the FP64 plain form at scale): a periodic water box of 8,192
 molecules = 24,576 atoms at 1.0 g/cm^3 (cubic, L = 118.26 bohr), seeded
@@ -11,11 +14,7 @@ functions per element (radial + narrow angular, cos cutoff 12 bohr), NN
 h2o_52).  One step = one frame through neighbor list, symmetry functions +
 dG/dr, atomic NNs + dE/dG, energy and forces, all in FP64.
 
-Metric: E+F atoms/s (higher is better).  `value` and `e2e` are the plain
-FP64 form; `forms` adds, on the same frames, the mixed-precision forms (FP32
-symmetry functions, tensor-core BF16 networks) for this potential and for
-the wider 92-SF / 64-64-64 potential, each with its speed-up over FP64 and
-its energy-per-atom and force RMSE against the FP64 form.
+Metric: E+F atoms/s (higher is better).
   value : device-resident frames (HBM), K steps between CUDA events on the
           library's stream, max over ranks; frames cycle through 100
           distinct coordinate sets and the per-frame working set (dG/dr,
@@ -24,6 +23,24 @@ its energy-per-atom and force RMSE against the FP64 form.
           the frame's positions host->device (pinned) and reads back energy
           and forces (n2p2b_set_positions / n2p2b_evaluate /
           n2p2b_get_forces / n2p2b_get_energy), wall clock around K steps.
+Further entries of the same line (one GPU):
+  forms   : the mixed-precision forms (FP32 symmetry functions, tensor-core
+            BF16 networks) and the gated student, on the same frames, for
+            this potential and the wider 92-SF / 64-64-64 one; speed-up over
+            FP64 and energy-per-atom / force RMSE against the FP64 form, and
+            whether each meets the stated targets; the gated student also on
+            compressed, noisier frames where it gates atoms to the teacher;
+  config4 : the precision form as specified: 98,304 atoms (32,768
+            molecules, L = 187.7 bohr), 92-SF / 64-64-64 softplus potential,
+            FP64 vs mixed atoms/s, RMSE against the FP64 form and against
+            the reference CPU library on one frame;
+  batch   : 4,096 structures of 33-513 atoms as one CUDA-graph launch, the
+            one-structure-per-call loop, and the largest per-structure
+            energy / force errors against the reference on a sample;
+  roofline: the dominant kernel (symmetry functions) against the FP64 pipe
+            (the bound: DGEMM peak measured in this run) with the HBM figure
+            beside it;
+  cpu_baseline: the reference library (OpenMP, all host cores) on 5 frames.
 
 Multi-GPU: one process per GPU (torchrun); each rank evaluates its own
 frames (independent replicas, weak scaling, no data-path collective); the
@@ -31,6 +48,10 @@ time is the max over ranks.
 
 --impl reference times the reference n2p2 CPU path (oracle/_ref, OpenMP on
 all host cores) on the same workload; each step is one full frame.
+
+--profile-case runs a small fixed evaluation (seed-77 water box, default
+4,096 molecules) and prints its per-stage device times; it is the command
+the ncu captures under profiles/ run.
 """
 from __future__ import annotations
 
@@ -53,17 +74,21 @@ POT_DIR = os.path.join(ROOT, "tests", "golden", "potentials")
 POT = os.path.join(POT_DIR, "h2o_52")
 STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
-# DRAM bytes (read + write) of one FP64 symmetry-function launch on this
-# workload: dram__bytes_read.sum + dram__bytes_write.sum = 0.570 + 2.500 GB,
-# measured by ncu on the launches of this very bench run (the launch list
-# summarized under profiles/).
-SF_TRAFFIC_BYTES = 3.070e9
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one FP64
+# symmetry-function launch on this workload, from the ncu capture
+# summarized in profiles/sfKernel_fp64_water12288.md (12,288-atom box,
+# scaled to 24,576 atoms by the number of neighbor entries).
+SF_TRAFFIC_BYTES = 2.24e9
+SF_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                     "the FP64 sfKernel, 12,288-atom box, x2.00 for 24,576 "
+                     "atoms (profiles/sfKernel_fp64_water12288.md)")
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
 SIGMA = 0.1
 METRIC = ("E+F atoms/s on 1 B200: plain FP64 vs BF16 / gated student at "
           "stated force RMSE")
+TARGETS = {"energy_per_atom_rmse": 1e-4, "force_rmse": 5e-3}
 
 
 def args():
@@ -73,11 +98,23 @@ def args():
     a.add_argument("--warmup", type=int, default=5)
     a.add_argument("--impl", choices=["ours", "reference"], default="ours")
     a.add_argument("--frames", type=int, default=N_FRAMES)
+    a.add_argument("--cpu-frames", type=int, default=5,
+                   help="frames of the in-line CPU baseline")
     a.add_argument("--no-cpu-baseline", action="store_true")
     a.add_argument("--no-forms", action="store_true",
-                   help="skip the mixed-precision comparison")
+                   help="skip the mixed-precision / student comparison")
+    a.add_argument("--no-config4", action="store_true",
+                   help="skip the 98,304-atom precision-form configuration")
     a.add_argument("--no-batch", action="store_true",
                    help="skip the 4,096-structure batching form")
+    # --profile-case
+    a.add_argument("--profile-case", action="store_true")
+    a.add_argument("--molecules", type=int, default=4096)
+    a.add_argument("--potential", default="h2o_52")
+    a.add_argument("--precision", default="fp64",
+                   choices=["fp64", "mixed", "bf16"])
+    a.add_argument("--evaluations", type=int, default=5)
+    a.add_argument("--autotune", action="store_true")
     return a.parse_args()
 
 
@@ -168,12 +205,31 @@ class ClockSampler:
 # ---------------------------------------------------------------------------
 # algorithmic work model (FLOPs and bytes per frame)
 # ---------------------------------------------------------------------------
-def work_model(cnt, index, dr, d, elem, rc=12.0):
+def potential_shape(p):
+    """Counting-model parameters of a set-up Prediction: angular members per
+    group M_a, radial members per group M_r, dG/dr slots per neighbor S,
+    SFs per element and NN multiply-adds per atom (first element)."""
+    M_a, M_r = 0, 0
+    for e in range(p.num_elements):
+        for g in p.symmetry_function_groups(e):
+            t = int(p.symmetry_function_params(e, g[0])[0])
+            if t == 2:
+                M_r = max(M_r, len(g))
+            else:
+                M_a = max(M_a, len(g))
+    S = max(p.num_slots(e, f) for e in range(p.num_elements)
+            for f in range(p.num_elements))
+    n_sf = max(p.num_symmetry_functions(e) for e in range(p.num_elements))
+    return M_a, M_r, S, n_sf
+
+
+def work_model(cnt, dr, d, shape, mac, rc=12.0):
     """Exact neighbor (n) and valid-triplet (T) counts of one frame and the
     FLOP / byte model: per triplet 40 + 60 M_a, per (pair, radial member)
     20, NN 3*2*MAC, chain rule 6 per stored Vec3D slot; bytes of the SF
     kernel = neighbor data read + dG/dr, G and dG/dr(self) written."""
     import torch
+    M_a, M_r, S, n_sf = shape
     dev = torch.device("cuda")
     N = len(cnt)
     off = np.concatenate([[0], np.cumsum(cnt)])
@@ -196,13 +252,12 @@ def work_model(cnt, index, dr, d, elem, rc=12.0):
         m = (dd < rc2) & ok[:, :, None] & ok[:, None, :] & tri
         T += int(m.sum())
     n = int(cnt.sum())
-    M_a, M_r, S, n_sf = 12, 8, 32, 52
-    mac = 52 * 25 + 25 * 25 + 25
     flops_sf = T * (40 + 60 * M_a) + n * M_r * 20
     flops_all = flops_sf + N * 3 * 2 * mac + 6 * (n * S + N * n_sf)
     bytes_sf = n * 32 + n * S * 3 * 8 + N * n_sf * 8 * 4 + N * 8 * 2
     return {"atoms": N, "neighbors": n, "triplets": T,
             "neighbors_per_atom": n / N, "triplets_per_atom": T / N,
+            "M_a": M_a, "M_r": M_r, "S": S, "n_sf": n_sf, "mac_nn": mac,
             "flops_sf": flops_sf, "flops_total": flops_all,
             "bytes_sf": bytes_sf}
 
@@ -239,10 +294,26 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def rmse_vs(acc, ref, n):
+    de = [(e - e0) / n for (e, _), (e0, _) in zip(acc, ref)]
+    df = np.concatenate([(f - f0).ravel() for (_, f), (_, f0) in zip(acc, ref)])
+    return (float(np.sqrt(np.mean(np.square(de)))),
+            float(np.sqrt(np.mean(np.square(df)))))
+
+
+def meets(entry, ref):
+    e = entry.get(f"energy_per_atom_rmse_vs_{ref}")
+    f = entry.get(f"force_rmse_vs_{ref}")
+    if e is None or f is None:
+        return None
+    return bool(e <= TARGETS["energy_per_atom_rmse"]
+                and f <= TARGETS["force_rmse"])
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline (reference library, OpenMP) -- rank 0, N = 1 only
 # ---------------------------------------------------------------------------
-def cpu_baseline(frames, box, elem, reps=1):
+def cpu_baseline(frames, box, elem, n_frames=5):
     from oracle import ref as oref
     lib = os.path.join(ROOT, "oracle", "_ref", "libn2p2ref_perf.so")
     if not os.path.exists(lib):
@@ -253,13 +324,16 @@ def cpu_baseline(frames, box, elem, reps=1):
     threads = os.cpu_count() or 1
     m = oref.RefModel(POT)
     m.setup_statistics()
-    m.set_structure(frames[0], elem, box)
-    t = m.time_stages(threads=threads, reps=reps)
+    t = np.zeros(5)
+    k = min(n_frames, len(frames))
+    for f in range(k):
+        m.set_structure(frames[f], elem, box)
+        t += m.time_stages(threads=threads, reps=1)
     total = float(t.sum())
-    natoms = len(elem) * reps
+    natoms = len(elem) * k
     return {"value": natoms / total, "unit": "atoms/s", "cores": threads,
             "kind": "reference",
-            "sample": f"{reps} frame(s) of the 24,576-atom box, full path "
+            "sample": f"{k} frames of the 24,576-atom box, full path "
                       "(neighbor list + SF + NN + E + F); stage seconds "
                       f"NL {t[0]:.2f}, SF {t[1]:.2f}, NN {t[2]:.2f}, "
                       f"E {t[3]:.4f}, F {t[4]:.2f}; without the O(N^2) "
@@ -349,14 +423,29 @@ def _stage_ms(p, frames_dev, steps):
     return [x / max(runs, 1) for x in ms]
 
 
+def _eval_frames(p, frames, box=None, elem=None):
+    """(energy, forces) of each frame (host arrays); a new box sets the
+    structure, otherwise only positions change."""
+    out = []
+    for x in frames:
+        if box is not None:
+            p.set_structure(x, elem, box)
+        else:
+            p.set_positions(x)
+        p.evaluate_nnp(True)
+        out.append((p.energy, p.forces().copy()))
+    return out
+
+
 def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
     """Plain FP64 vs the mixed forms on the same 24,576-atom frames, for the
     52-SF potential and the wider 92-SF / 64-64-64 softplus potential, and
     for the latter the distilled 92-32-1 student (gated by its training
     range; atoms outside it are re-evaluated by the teacher on the tensor
     cores).  Accuracy is measured against the FP64 form on three frames (the
-    FP64 form equals the reference to 1e-10, tests/test_gpu_parity.py) and,
-    for the student, also against the mixed-precision teacher."""
+    FP64 form equals the reference to 1e-10 on this very workload,
+    tests/test_gpu_bench_parity.py) and, for the student, also against the
+    mixed-precision teacher."""
     from n2p2_b200.mode import Prediction
     n = len(elem)
     out = {}
@@ -369,7 +458,9 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
         forms = [("fp64", "fp64", None), ("mixed", "mixed", None),
                  ("bf16", "bf16", None)]
         sdir = os.path.join(POT_DIR, pot + "_student")
-        if os.path.exists(os.path.join(sdir, "training_range.data")):
+        has_student = os.path.exists(os.path.join(sdir,
+                                                  "training_range.data"))
+        if has_student:
             p.setup_student(sdir)
             forms += [("student_gated", "mixed", "gated"),
                       ("student_only", "mixed", "only")]
@@ -377,8 +468,8 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
         tunes = {}
         for name, prec, smode in forms:
             p.set_precision(prec)
-            if smode is not None:
-                p.set_student_mode(smode)
+            if has_student:
+                p.set_student_mode(smode if smode else "off")
             p.set_positions(frames[0])
             p.evaluate_nnp(True)
             if prec not in tunes:
@@ -389,12 +480,12 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
             p.finish()
             t, launches = _time_steps(p, dev_frames, steps, stream, lib)
             stage = _stage_ms(p, dev_frames, min(steps, 10))
-            acc, gated = [], []
-            for s in range(3):
-                p.set_positions(frames[s])
-                p.evaluate_nnp(True)
-                acc.append((p.energy, p.forces().copy()))
-                if smode == "gated":
+            acc = _eval_frames(p, frames[:3])
+            gated = []
+            if smode == "gated":
+                for s in range(3):
+                    p.set_positions(frames[s])
+                    p.evaluate_nnp(True)
                     gated.append(p.student_gated_count() / n)
             entry = {"value": n * steps / t, "unit": "atoms/s",
                      "ms_per_step": 1e3 * t / steps, "steps": steps,
@@ -405,44 +496,165 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
             for rname in (("fp64", "mixed") if smode else ("fp64",)):
                 if name == rname:
                     continue
-                ref = refs[rname]
-                de = [(e - e0) / n for (e, _), (e0, _) in zip(acc, ref)]
-                df = np.concatenate([(f - f0).ravel()
-                                     for (_, f), (_, f0) in zip(acc, ref)])
-                entry[f"energy_per_atom_rmse_vs_{rname}"] = float(
-                    np.sqrt(np.mean(np.square(de))))
-                entry[f"force_rmse_vs_{rname}"] = float(
-                    np.sqrt(np.mean(np.square(df))))
+                e_r, f_r = rmse_vs(acc, refs[rname], n)
+                entry[f"energy_per_atom_rmse_vs_{rname}"] = e_r
+                entry[f"force_rmse_vs_{rname}"] = f_r
             if name != "fp64":
                 entry["speedup_vs_fp64"] = (
                     entry["value"] / out[pot]["fp64"]["value"])
+                entry["meets_targets"] = meets(entry, "fp64")
             if gated:
                 entry["gated_fraction"] = float(np.mean(gated))
             out.setdefault(pot, {})[name] = entry
         out[pot]["force_rms"] = float(
             np.sqrt(np.mean(np.square(refs["fp64"][0][1]))))
+        if has_student:
+            out[pot]["student_gated_compressed"] = measure_gated_compressed(
+                p, box, elem, stream, lib, steps)
         p.close()
-    out["targets"] = {"energy_per_atom_rmse": 1e-4, "force_rmse": 5e-3,
-                      "units": "potential energy units; energy / bohr"}
+    out["targets"] = dict(TARGETS, units="potential energy units; energy / "
+                                         "bohr")
     out["forms"] = {
         "fp64": "plain form, everything FP64",
         "mixed": "FP32 symmetry functions + dG/dr; NN on tcgen05 with BF16 "
                  "hi/lo operand pairs (3 MMAs per step), FP32 accumulation; "
                  "FP64 displacements, energy sum, force accumulation",
-        "bf16": "as mixed with single BF16 operands (1 MMA per step)",
+        "bf16": "as mixed with single BF16 operands (1 MMA per step); "
+                "meets_targets says whether its RMSE is inside the targets",
         "student_gated": "FP32 symmetry functions; distilled 92-32-1 FP32 "
                          "student for atoms inside its training range, the "
                          "mixed-precision teacher for the others",
-        "student_only": "the student for every atom (no gate)"}
+        "student_only": "the student for every atom (no gate)",
+        "student_gated_compressed": "the gated student on frames outside "
+                                    "its training distribution (box and "
+                                    "positions compressed by 5 %, noise "
+                                    "sigma 0.25 bohr), where the gate hands "
+                                    "atoms to the teacher"}
     return out
 
 
-def measure_batch(stream, lib, local, n_structures=4096, steps=5):
+def measure_gated_compressed(p, box, elem, stream, lib, steps):
+    """The gated student (its Prediction already set up) on frames the
+    student was not trained for -- compressed by 5 % with sigma = 0.25 bohr
+    noise (its training used +-3 % and sigma <= 0.2) -- so that a part of the
+    atoms falls outside its training range and goes to the teacher.  Speed
+    with that gated fraction, and accuracy against the FP64 form."""
+    import torch
+    from n2p2_b200 import synth
+    n = len(elem)
+    s = 0.95
+    bx = box * s
+    _, pos0, _ = synth.water_box(N_MOL, SEED)
+    _, fr = synth.noisy_frames(pos0 * s, 12, 0.25, seed=SEED + 77)
+    dev = torch.tensor(fr, dtype=torch.float64, device="cuda")
+    p.set_precision("fp64")
+    p.set_student_mode("off")
+    ref = _eval_frames(p, fr[:3], bx, elem)
+    p.set_precision("mixed")
+    p.set_student_mode("gated")
+    p.set_structure(fr[0], elem, bx)
+    p.evaluate_nnp(True)
+    for k in range(3):
+        p.set_positions(dev[k])
+        p.evaluate_async(True)
+    p.finish()
+    t, launches = _time_steps(p, dev, steps, stream, lib)
+    acc, gated = [], []
+    for k in range(3):
+        p.set_positions(fr[k])
+        p.evaluate_nnp(True)
+        acc.append((p.energy, p.forces().copy()))
+        gated.append(p.student_gated_count() / n)
+    e_r, f_r = rmse_vs(acc, ref, n)
+    entry = {"value": n * steps / t, "unit": "atoms/s",
+             "ms_per_step": 1e3 * t / steps, "steps": steps,
+             "gated_fraction": float(np.mean(gated)),
+             "energy_per_atom_rmse_vs_fp64": e_r, "force_rmse_vs_fp64": f_r,
+             "frames": "box x0.95, sigma 0.25 bohr, 12 frames"}
+    entry["meets_targets"] = meets(entry, "fp64")
+    p.set_student_mode("off")
+    return entry
+
+
+def measure_config4(stream, lib, local, steps=10):
+    """The precision form as specified: 32,768 water molecules = 98,304
+    atoms (L = 187.7 bohr at 1.0 g/cm^3), the 92-SF / 64-64-64 softplus
+    potential (h2o_92), three noisy frames (sigma 0.1 bohr).  FP64 vs mixed
+    atoms/s (device-resident frames), per-atom energy and force RMSE of the
+    mixed form against the FP64 form (3 frames) and of both against the
+    reference CPU library on the first frame."""
+    import torch
+    from n2p2_b200 import synth
+    from n2p2_b200.mode import Prediction
+    pot = os.path.join(POT_DIR, "h2o_92")
+    t0 = time.perf_counter()
+    box, pos, elem = synth.water_box(32768, 2030)
+    _, fr = synth.noisy_frames(pos, 3, SIGMA, seed=2031, box=box)
+    gen = time.perf_counter() - t0
+    n = len(elem)
+    dev = torch.tensor(fr, dtype=torch.float64, device="cuda")
+    p = Prediction(pot, device=local)
+    p.setup()
+    p.setup_symmetry_function_statistics(False, False, False, False)
+    p.set_stream(stream.cuda_stream)
+    out = {"atoms": n, "box_bohr": float(box[0, 0]),
+           "potential": "h2o_92: 92 SFs/element, NN 92-64-64-64-1 softplus",
+           "generation_s": gen}
+    res = {}
+    for prec in ("fp64", "mixed"):
+        p.set_precision(prec)
+        p.set_structure(fr[0], elem, box)
+        p.evaluate_nnp(True)
+        tune = p.autotune(True, 1)
+        for k in range(3):
+            p.set_positions(dev[k])
+            p.evaluate_async(True)
+        p.finish()
+        t, _ = _time_steps(p, dev, steps, stream, lib)
+        stage = _stage_ms(p, dev, 3)
+        res[prec] = _eval_frames(p, fr)
+        out[prec] = {"value": n * steps / t, "unit": "atoms/s",
+                     "ms_per_step": 1e3 * t / steps, "steps": steps,
+                     "stage_ms_per_step": dict(zip(STAGES, stage)),
+                     "autotune": tune}
+    p.close()
+    e_r, f_r = rmse_vs(res["mixed"], res["fp64"], n)
+    out["mixed"]["energy_per_atom_rmse_vs_fp64"] = e_r
+    out["mixed"]["force_rmse_vs_fp64"] = f_r
+    out["mixed"]["speedup_vs_fp64"] = (out["mixed"]["value"]
+                                       / out["fp64"]["value"])
+    out["mixed"]["meets_targets"] = meets(out["mixed"], "fp64")
+    from oracle import ref as oref
+    if oref.ref_available():
+        t0 = time.perf_counter()
+        ref = oref.RefModel(pot)
+        ref.setup_statistics()
+        ref.set_structure(fr[0], elem, box)
+        e0, f0 = ref.predict()
+        out["reference_frame_s"] = time.perf_counter() - t0
+        for prec in ("fp64", "mixed"):
+            e_r, f_r = rmse_vs(res[prec][:1], [(e0, f0)], n)
+            out[prec]["energy_per_atom_rmse_vs_reference"] = e_r
+            out[prec]["force_rmse_vs_reference"] = f_r
+        e, f = res["fp64"][0]
+        scale = np.maximum(np.abs(f0), np.sqrt(np.mean(f0 ** 2)))
+        out["fp64"]["relative_energy_error_vs_reference"] = abs(e - e0) / abs(
+            e0)
+        out["fp64"]["max_force_error_vs_reference"] = float(
+            (np.abs(f - f0) / scale).max())
+        del ref
+    return out
+
+
+def measure_batch(stream, lib, local, n_structures=4096, steps=5,
+                  check=64):
     """Batching form: 4,096 independent water boxes of 11-171 molecules
     (33-513 atoms, density 1.0 g/cm^3), evaluated together as one CUDA-graph
     launch after the autotuner picked the launch configuration for their
     size bucket (tuned on a 256-structure sample of the same distribution).
-    Compared with a loop that evaluates one structure per call."""
+    Compared with a loop that evaluates one structure per call.  The FP64
+    batch result of `check` structures (the largest and smallest included)
+    is compared with the reference library, structure by structure."""
     import torch
     from n2p2_b200 import synth
     from n2p2_b200.mode import Prediction
@@ -451,9 +663,9 @@ def measure_batch(stream, lib, local, n_structures=4096, steps=5):
     sample = synth.batch_structures(256, 2028, device=f"cuda:{local}")
     gen_s = time.perf_counter() - t0
     natoms = sum(len(s[2]) for s in structs)
+    sizes = np.array([len(s[2]) for s in structs])
     out = {"structures": n_structures, "atoms": natoms,
-           "atoms_per_structure": [int(min(len(s[2]) for s in structs)),
-                                   int(max(len(s[2]) for s in structs))],
+           "atoms_per_structure": [int(sizes.min()), int(sizes.max())],
            "generation_s": gen_s}
     p = Prediction(POT, device=local)
     p.setup()
@@ -466,6 +678,9 @@ def measure_batch(stream, lib, local, n_structures=4096, steps=5):
         tune = p.autotune(True, 1)
         p.set_structures(structs)
         p.evaluate_nnp(True)
+        if prec == "fp64":
+            E = p.structure_energies()
+            F = p.forces()
         p.capture_graph(True)
         p.launch_graph()
         p.finish()
@@ -481,9 +696,34 @@ def measure_batch(stream, lib, local, n_structures=4096, steps=5):
         out[prec] = {"value": natoms * steps / t, "unit": "atoms/s",
                      "ms_per_batch": 1e3 * t / steps, "steps": steps,
                      "graph_launches_per_batch": 1,
-                     "kernels_per_batch": (lib.n2p2b_kernel_launch_count()
-                                           - l0) / steps,
+                     "kernels_per_graph": "the evaluation pipeline "
+                                          "(captured once; replays are not "
+                                          "counted as launches)",
                      "autotune": tune}
+    # Per-structure errors of the FP64 batch against the reference.
+    from oracle import ref as oref
+    if oref.ref_available():
+        ref = oref.RefModel(POT)
+        ref.setup_statistics()
+        off = np.concatenate([[0], np.cumsum(sizes)])
+        pick = sorted(set([int(sizes.argmax()), int(sizes.argmin())]
+                          + list(np.random.default_rng(5).choice(
+                              n_structures, check - 2, replace=False))))
+        we, wf = 0.0, 0.0
+        for s in pick:
+            box, x, el = structs[s]
+            ref.set_structure(x, el, box)
+            e0, f0 = ref.predict()
+            f = F[off[s]:off[s + 1]]
+            scale = np.maximum(np.abs(f0), np.sqrt(np.mean(f0 ** 2)))
+            we = max(we, abs(E[s] - e0) / abs(e0))
+            wf = max(wf, float((np.abs(f - f0) / scale).max()))
+        out["fp64"]["reference_check"] = {
+            "structures": len(pick),
+            "atoms_range": [int(sizes[pick].min()), int(sizes[pick].max())],
+            "max_relative_energy_error": we,
+            "max_force_error": wf,
+            "force_error_measure": "|dF| / max(|F|, rms F) per component"}
     # One structure per call (set_structure + evaluate), on a sample.
     p.set_precision("fp64")
     k = 512
@@ -565,15 +805,17 @@ def run_ours(a):
 
         # ---- profiled pass: per-stage device time -------------------------
         per = _stage_ms(p, dev_frames, a.steps)
+    clock_summary = clocks.summary()
 
-        # ---- the other forms (one GPU only) -------------------------------
-        forms = None
-        if world == 1 and not a.no_forms:
-            forms = measure_forms(box, frames, elem, dev_frames, stream, lib,
-                                  min(a.steps, 50), local)
-        batch = None
-        if world == 1 and not a.no_batch:
-            batch = measure_batch(stream, lib, local)
+    # ---- the other forms and configurations (one GPU only) ----------------
+    forms = config4 = batch = None
+    if world == 1 and not a.no_forms:
+        forms = measure_forms(box, frames, elem, dev_frames, stream, lib,
+                              min(a.steps, 50), local)
+    if world == 1 and not a.no_config4:
+        config4 = measure_config4(stream, lib, local)
+    if world == 1 and not a.no_batch:
+        batch = measure_batch(stream, lib, local)
 
     rep.barrier()
 
@@ -588,7 +830,8 @@ def run_ours(a):
     p.set_positions(dev_frames[0])
     p.evaluate_nnp(True)
     cnt, index, dr, d = p.neighbor_list()
-    wm = work_model(cnt, index, dr, d, elem)
+    mac = 52 * 25 + 25 * 25 + 25
+    wm = work_model(cnt, dr, d, potential_shape(p), mac)
     sf_s = per[1] / 1e3
     hbm_peak, peak_kind = measured_peaks()
     gbs = wm["bytes_sf"] / sf_s / 1e9
@@ -610,35 +853,79 @@ def run_ours(a):
         "gpu_launches": launches,
         "stage_ms_per_step": dict(zip(STAGES, per)),
         "autotune": tune,
-        "roofline": {"kernel": "sfKernel<double> (symmetry functions + "
-                               "dG/dr)",
-                     "bound": "hbm", "achieved": gbs, "peak": hbm_peak,
-                     "unit": "GB/s", "frac": gbs / hbm_peak,
-                     "peak_source": peak_kind,
-                     "traffic": SF_TRAFFIC_BYTES,
-                     "algorithmic_bytes_per_launch": wm["bytes_sf"]},
-        "roofline_fp64": {"kernel": "sfKernel<double>", "achieved": sf_tflops,
-                          "peak": fp64_peak, "unit": "TFLOP/s",
-                          "frac": sf_tflops / fp64_peak,
-                          "peak_source": "cuBLAS DGEMM 8192^3 measured here",
-                          "algorithmic_flops_per_launch": wm["flops_sf"]},
+        "roofline": {
+            "kernel": "sfKernel<double> (symmetry functions + dG/dr)",
+            "bound": "fp64",
+            "achieved": sf_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
+            "frac": sf_tflops / fp64_peak,
+            "peak_source": "cuBLAS DGEMM 8192^3 timed in this run "
+                           "(builder-measured: the driver's peaks file has "
+                           "no FP64 figure)",
+            "achieved_source": "counting-model FLOPs of the frame (exact "
+                               "triplet and neighbor counts, see work) / "
+                               "the SF stage's CUDA-event time",
+            "algorithmic_flops_per_launch": wm["flops_sf"],
+            "traffic": SF_TRAFFIC_BYTES,
+            "traffic_source": SF_TRAFFIC_SOURCE,
+            "hbm": {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
+                    "frac": gbs / hbm_peak,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json "
+                                   "hbm_gbs)",
+                    "algorithmic_bytes_per_launch": wm["bytes_sf"]}},
         "work": wm,
         "energy_last_frame": energy,
-        "clocks": clocks.summary(),
+        "clocks": clock_summary,
     }
     if forms is not None:
         line["forms"] = forms
+    if config4 is not None:
+        line["config4"] = config4
     if batch is not None:
         line["batch"] = batch
     if not a.no_cpu_baseline and world == 1:
-        line["cpu_baseline"] = cpu_baseline(frames, box, elem)
+        line["cpu_baseline"] = cpu_baseline(frames, box, elem, a.cpu_frames)
     print(json.dumps(line))
     rep.close()
 
 
+def profile_case(a):
+    """A small fixed evaluation for profilers and quick timings: a seed-77
+    water box of --molecules molecules on one of the test potentials,
+    --evaluations evaluations (energy + forces); prints the per-stage
+    device times of the last three.  The symmetry-function kernel of
+    evaluation k is that kernel's launch k (the first evaluation's sizing
+    pass launches the neighbor list only).  --autotune runs the library's
+    tuner first and prints its choice; a capture that should see launch k
+    passes that choice through N2P2B_SF_VARIANT / N2P2B_SF_SORT instead,
+    because the tuner launches every configuration."""
+    from n2p2_b200 import synth
+    from n2p2_b200.mode import Prediction
+    box, pos, elem = synth.water_box(a.molecules, 77)
+    p = Prediction(os.path.join(POT_DIR, a.potential))
+    p.setup()
+    p.setup_symmetry_function_statistics(False, False, False, False)
+    p.set_precision(a.precision)
+    p.set_structure(pos, elem, box)
+    if a.autotune:
+        p.evaluate_nnp(True)
+        print("autotune", p.autotune(True, 3))
+    for _ in range(max(a.evaluations - 3, 1)):
+        p.evaluate_nnp(True)
+    p.set_profiling(True)
+    p.stage_times(True)
+    for _ in range(3):
+        p.evaluate_nnp(True)
+    ms, runs = p.stage_times(True)
+    print(a.potential, a.precision, len(elem), "atoms; stage ms "
+          "(NL, SF, NN, E, F):", [round(x / runs, 3) for x in ms],
+          "energy", p.energy)
+
+
 def main():
     a = args()
-    if a.impl == "reference":
+    if a.profile_case:
+        profile_case(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

@@ -360,7 +360,10 @@ uint64_t n2p2b_kernel_launch_count(void);
  * must start at zero), so calls whose GPU work overlaps (other streams or
  * host threads) race: serialize them.  The first call for a device looks up
  * the array's device address (cudaGetSymbolAddress) and should come before
- * any stream capture.
+ * any stream capture.  With CUDA's lazy module loading (the default) that
+ * first call also loads the library's device code and the array onto the
+ * device, which needs device memory: make one warm-up call before the host
+ * reserves its GPU memory, or run with CUDA_MODULE_LOADING=EAGER.
  *
  * device:    CUDA device to run on (the caller's current device is kept).
  * stream:    cudaStream_t for the work (NULL = default stream); the call
@@ -371,7 +374,9 @@ uint64_t n2p2b_kernel_launch_count(void);
  * offsets:   device, num_atoms + 1      exclusive prefix of counts (output)
  * index, dr, d: device, capacity, 3 x capacity, capacity: neighbor index,
  *            displacement r_i - r_j + image and distance (output).
- * total:     host, number of entries (also when capacity was too small).
+ * total:     host, number of entries (also when capacity was too small;
+ *            lists of more than 2^31 - 1 entries do not fit the int32
+ *            offsets and are rejected with N2P2B_ERR_CAPACITY).
  * err:       optional host buffer for a message. */
 #define N2P2B_NOALLOC_MAX_ATOMS      65536
 #define N2P2B_NOALLOC_MAX_NEIGHBORS  1024

@@ -510,6 +510,7 @@ public:
         dr_.clear();
         pending_.assign(elements_.size(), {});
         maxTarget_ = numAtomsLocal;
+        finalized_ = false;
     }
     void setLocalTags(int const* const) {}
     void setLocalTags(int64_t const* const) {}
@@ -532,9 +533,15 @@ public:
             Entry{j, it->second, dx * cflength_, dy * cflength_,
                   dz * cflength_});
         if (j + 1 > maxTarget_) maxTarget_ = j + 1;
+        finalized_ = false;
     }
+    // InterfaceLammps::finalizeNeighborList (InterfaceLammps.cpp:444-461):
+    // the reference needs it only for 4G potentials, and the 2G pair style
+    // never calls it (pair_hdnnp.cpp:81-120), so process() runs it itself
+    // when neighbors were added since the last call.
     void finalizeNeighborList()
     {
+        finalized_ = true;
         index_.clear();
         nelem_.clear();
         dr_.clear();
@@ -553,6 +560,7 @@ public:
     // InterfaceLammps::process (libnnpif/LAMMPS/InterfaceLammps.cpp:463-487)
     void process()
     {
+        if (!finalized_) finalizeNeighborList();
         if (elements_.empty()) return;
         if (resetew_) resetExtrapolationWarnings();
         check(ctx_, n2p2b_set_neighbor_list(ctx_, (int64_t)elements_.size(),
@@ -608,12 +616,15 @@ public:
     // SymFncStatistics::clear on every element: the warnings and their count.
     void clearExtrapolationWarnings() { resetExtrapolationWarnings(); }
 
-    // In LAMMPS units.
+    // InterfaceLammps::getMaxCutoffRadius (InterfaceLammps.cpp:489-493):
+    // the largest symmetry-function cutoff in LAMMPS units (the pair style
+    // checks its own cutoff against it, pair_hdnnp.cpp:245).
+    double getMaxCutoffRadius() const { return getMaxCutoffRadiusLammps(); }
     double getMaxCutoffRadiusLammps() const
     {
         double meanE, convE, convL;
         n2p2b_unit_conversion(ctx_, &meanE, &convE, &convL);
-        return getMaxCutoffRadius() / convL / cflength_;
+        return Mode::getMaxCutoffRadius() / convL / cflength_;
     }
 
 private:
@@ -624,6 +635,7 @@ private:
         double dx, dy, dz;
     };
     bool                            initialized_ = false;
+    bool                            finalized_ = false;
     bool                            showew_ = false, resetew_ = false;
     int                             maxew_ = 0;
     double                          cflength_ = 1.0, cfenergy_ = 1.0;

@@ -24,7 +24,12 @@
 // In host code the array's name is only a host-side stand-in; its device
 // address is obtained once per device with cudaGetSymbolAddress (with that
 // device current) on the first call made for the device, so that first call
-// should come before any stream capture.
+// should come before any stream capture.  Under CUDA's lazy module loading
+// (the default) that first call is also when the library's device code and
+// this array are loaded onto the device, which takes device memory: make
+// one warm-up call before the host reserves its memory (or set
+// CUDA_MODULE_LOADING=EAGER).  Every call waits on the host until its
+// stream has finished the work (it reads the status words back).
 #include "n2p2_b200.h"
 
 #include <cuda_runtime.h>
@@ -54,8 +59,9 @@ constexpr unsigned kFull = 0xffffffffu;
 enum
 {
     S_FLAGS = 0,
-    S_TOTAL = 1,
-    S_MAXNBR = 2
+    S_TOTAL_LO = 1,   // total entries, low and high 32 bits (unclamped)
+    S_TOTAL_HI = 2,
+    S_MAXNBR = 3
 };
 enum
 {
@@ -175,9 +181,14 @@ __global__ void naScan(int n, int const* __restrict__ cnt,
         off[n] = (int)min(run, (long)0x7fffffff);
         if (record)
         {
-            status[S_TOTAL] = (int)min(run, (long)0x7fffffff);
+            unsigned long long const u = (unsigned long long)run;
+            status[S_TOTAL_LO] = (int)(unsigned)(u & 0xffffffffull);
+            status[S_TOTAL_HI] = (int)(unsigned)(u >> 32);
             status[S_MAXNBR] = m;
-            if (run > capacity) status[S_FLAGS] |= F_OVERFLOW;
+            // Offsets and indices are int32: a list of more than INT32_MAX
+            // entries cannot be written, whatever the caller's capacity.
+            if (run > capacity || run > 0x7fffffffL)
+                status[S_FLAGS] |= F_OVERFLOW;
             if (m > kMaxNeighbors) status[S_FLAGS] |= F_TOO_MANY_NEIGHBORS;
         }
     }
@@ -510,12 +521,17 @@ extern "C" int n2p2b_neighbor_list_noalloc(
     cudaSetDevice(prev);
     if (e != cudaSuccess)
         return fail(err, err_len, N2P2B_ERR_CUDA, cudaGetErrorString(e));
-    *total = stat[S_TOTAL];
+    *total = (int64_t)(((unsigned long long)(unsigned)stat[S_TOTAL_HI] << 32)
+                       | (unsigned long long)(unsigned)stat[S_TOTAL_LO]);
     if ((stat[S_FLAGS] & F_TOO_MANY_NEIGHBORS) && cellPath
         && !(stat[S_FLAGS] & F_OUTSIDE))
         return fail(err, err_len, N2P2B_ERR_CAPACITY,
                     "n2p2b_neighbor_list_noalloc: an atom has more than "
                     "N2P2B_NOALLOC_MAX_NEIGHBORS (1024) neighbors");
+    if ((stat[S_FLAGS] & F_OVERFLOW) && *total > 0x7fffffffLL)
+        return fail(err, err_len, N2P2B_ERR_CAPACITY,
+                    "n2p2b_neighbor_list_noalloc: more than 2^31 - 1 entries "
+                    "(int32 offsets); *total holds the number of entries");
     if (stat[S_FLAGS] & F_OVERFLOW)
         return fail(err, err_len, N2P2B_ERR_CAPACITY,
                     "n2p2b_neighbor_list_noalloc: output capacity too small "

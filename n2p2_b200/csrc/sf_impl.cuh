@@ -266,6 +266,67 @@ __device__ __forceinline__ R powInt16(R x, int n)
     return result;
 }
 
+// x^m for a run multiple 1 <= m <= 1024 (exponentiation by squaring; lanes
+// of a round share m, so the loop does not diverge).
+template <typename R>
+__device__ __forceinline__ R powMult(R x, int m)
+{
+    R result = R(1);
+    unsigned k = (unsigned)m;
+    while (true)
+    {
+        if (k & 1u) result *= x;
+        k >>= 1;
+        if (k == 0u) break;
+        x *= x;
+    }
+    return result;
+}
+
+// Inverse factorials 1 / n! as compile-time constants.
+template <int N>
+struct InvFact
+{
+    static constexpr double value = InvFact<N - 1>::value / double(N);
+};
+template <>
+struct InvFact<0>
+{
+    static constexpr double value = 1.0;
+};
+
+// Horner steps n = N .. 0 of sum_n (-1)^n v^n / (2n + K)!  (K = 0: cos,
+// K = 1: sin(x) / x, with x^2 = v).
+template <int N, int K>
+struct AltSeries
+{
+    __device__ static __forceinline__ double run(double v, double acc)
+    {
+        constexpr double c = ((N & 1) ? -1.0 : 1.0) * InvFact<2 * N + K>::value;
+        return AltSeries<N - 1, K>::run(v, fma(acc, v, c));
+    }
+};
+template <int K>
+struct AltSeries<-1, K>
+{
+    __device__ static __forceinline__ double run(double, double acc)
+    {
+        return acc;
+    }
+};
+
+// The cosine cutoff (alpha = 0) of a pair distance r from v = (a r)^2,
+// a = pi / rc, without a square root or sin / cos: the Taylor series
+//   cos(a r)          = sum_{n>=0} (-1)^n v^n / (2n)!
+//   sin(a r) / (a r)  = sum_{n>=0} (-1)^n v^n / (2n + 1)!
+// by Horner's rule.  For 0 <= v <= pi^2 (r <= rc) the first omitted terms
+// are below 3.1e-18 (cos, n = 16) and 9.4e-18 (sin / x, n = 15).
+__device__ __forceinline__ void cosSincSeries(double v, double& c, double& s)
+{
+    c = AltSeries<15, 0>::run(v, 0.0);
+    s = AltSeries<14, 1>::run(v, 0.0);
+}
+
 // Per-warp shared-memory views.
 template <typename R>
 struct WarpMem
@@ -1165,6 +1226,7 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                     aPz[r][s] = R(0);
                 }
             R eta2[NRC], etaN[NRC];
+            int emul[NRC];
             R const* Er[NRC];
 #pragma unroll
             for (int r = 0; r < NRC; ++r)
@@ -1173,8 +1235,17 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                 DevMember const& mm = M[g.mbeg + rr * NS];
                 eta2[r] = R(2) * R(mm.eta);
                 etaN[r] = -R(mm.eta);
+                emul[r] = mm.etaMult;
                 Er[r] = W.E + (long)mm.expIdx * capE;
             }
+            // FP64: r_jk's cutoff from a power series in r_jk^2 and one
+            // exponential for all runs when their etas are integer
+            // multiples of the smallest (see cosSincSeries, DevGroup).
+            bool const series = (sizeof(R) == 8) && (CT == 1) && NARROW
+                              && g.cosSeries;
+            bool const chain = (sizeof(R) == 8) && NARROW && g.expChain;
+            R const a2 = R(g.a2);
+            R const etaB = -R(g.etaBase);
             if (valid && rb < nr)
             {
                 R const cr0 = invij * invij;  // 1 / r_ij^2
@@ -1211,12 +1282,26 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                         {
                             r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1]
                                + dr3[2] * dr3[2];
-                            R const invjk = mrsqrt(r2);
-                            R pfcjk, pdfcjk;
-                            cutoffFdf<R, CT>(P, g, r2 * invjk, pfcjk, pdfcjk);
+                            // f_c(r_jk) and f_c'(r_jk) / r_jk
+                            R pfcjk, qjk;
+                            if (series)
+                            {
+                                double c, sc;
+                                cosSincSeries((double)(a2 * r2), c, sc);
+                                pfcjk = R(0.5) * R(c) + R(0.5);
+                                qjk = R(-0.5) * a2 * R(sc);
+                            }
+                            else
+                            {
+                                R const invjk = mrsqrt(r2);
+                                R pdfcjk;
+                                cutoffFdf<R, CT>(P, g, r2 * invjk, pfcjk,
+                                                 pdfcjk);
+                                qjk = pdfcjk * invjk;
+                            }
                             pfc = pfcij * pfcik * pfcjk;
                             pr1 = pfcik * pfcjk * pdfcrij;
-                            pr3 = pfcij * pfcik * pdfcjk * invjk;
+                            pr3 = pfcij * pfcik * qjk;
                         }
                         else
                         {
@@ -1241,11 +1326,26 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                             Z1[s] = zl[s] * X1;
                             Z3[s] = zl[s] * X3;
                         }
+                        // exp(-eta_r r_jk^2) per run
+                        R ejk[NRC];
+                        if (NARROW && chain)
+                        {
+                            R const b = mexp(etaB * r2);
+#pragma unroll
+                            for (int r = 0; r < NRC; ++r)
+                                ejk[r] = powMult(b, emul[r]);
+                        }
+                        else if (NARROW)
+                        {
+#pragma unroll
+                            for (int r = 0; r < NRC; ++r)
+                                ejk[r] = mexp(etaN[r] * r2);
+                        }
 #pragma unroll
                         for (int r = 0; r < NRC; ++r)
                         {
                             R vexp = Er[r][t] * Er[r][k];
-                            if (NARROW) vexp *= mexp(etaN[r] * r2);
+                            if (NARROW) vexp *= ejk[r];
                             R const e2p = eta2[r] * pfc;
                             R const Y1 = pr1 - e2p;
                             R const Y3 = NARROW ? e2p - pr3 : R(0);
