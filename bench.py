@@ -76,12 +76,14 @@ STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one FP64
 # symmetry-function launch on this workload, from the ncu capture
-# summarized in profiles/sfKernel_fp64_water12288.md (12,288-atom box,
-# scaled to 24,576 atoms by the number of neighbor entries).
-SF_TRAFFIC_BYTES = 2.24e9
+# summarized in profiles/sfKernel_fp64_fp32_water12288.md (12,288-atom box,
+# 1.512 GB), scaled to the 24,576-atom frame by its neighbor entries
+# (x 2.002).
+SF_TRAFFIC_BYTES = 3.027e9
 SF_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                     "the FP64 sfKernel, 12,288-atom box, x2.00 for 24,576 "
-                     "atoms (profiles/sfKernel_fp64_water12288.md)")
+                     "the FP64 sfKernel on the 12,288-atom box (1.512 GB), "
+                     "x 2.002 neighbor entries for 24,576 atoms "
+                     "(profiles/sfKernel_fp64_fp32_water12288.md)")
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
@@ -115,6 +117,9 @@ def args():
                    choices=["fp64", "mixed", "bf16"])
     a.add_argument("--evaluations", type=int, default=5)
     a.add_argument("--autotune", action="store_true")
+    a.add_argument("--student-steps", type=int, default=0,
+                   help="--profile-case: that many training steps of the "
+                        "distilled student (h2o_92_student) instead")
     return a.parse_args()
 
 
@@ -901,6 +906,8 @@ def profile_case(a):
     from n2p2_b200 import synth
     from n2p2_b200.mode import Prediction
     box, pos, elem = synth.water_box(a.molecules, 77)
+    if a.student_steps:
+        return profile_student(a, box, pos, elem)
     p = Prediction(os.path.join(POT_DIR, a.potential))
     p.setup()
     p.setup_symmetry_function_statistics(False, False, False, False)
@@ -919,6 +926,47 @@ def profile_case(a):
     print(a.potential, a.precision, len(elem), "atoms; stage ms "
           "(NL, SF, NN, E, F):", [round(x / runs, 3) for x in ms],
           "energy", p.energy)
+
+
+def profile_student(a, box, pos, elem):
+    """--profile-case --student-steps K: K Adam steps of the distilled
+    92-32-1 student (tests/golden/potentials/h2o_92_student, in memory
+    only) on batches of 4,096 atoms of one frame labelled by its FP64
+    teacher; prints the device time per step."""
+    import torch
+    from n2p2_b200.mode import Prediction
+    teacher = os.path.join(POT_DIR, "h2o_92")
+    t = Prediction(teacher)
+    t.setup()
+    t.setup_symmetry_function_statistics(False, False, False, False)
+    t.set_structure(pos, elem, box)
+    t.evaluate_nnp(True)
+    E = torch.tensor(t.atomic_energies(), dtype=torch.float64, device="cuda")
+    F = torch.tensor(t.forces(), dtype=torch.float64, device="cuda")
+    t.close()
+    p = Prediction(teacher)
+    p.setup()
+    p.setup_symmetry_function_statistics(False, False, False, False)
+    p.set_precision("mixed")
+    p.setup_student(os.path.join(POT_DIR, "h2o_92_student"))
+    p.set_structure(pos, elem, box)
+    p.calculate_neighbor_list()
+    p.calculate_symmetry_function_groups(True)
+    n = len(elem)
+    idx = torch.arange(min(4096, n), dtype=torch.int32, device="cuda")
+    for _ in range(3):
+        p.student_train_step(E, F, idx, 1.0, 1.0, 1e-6)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(a.student_steps):
+        p.student_train_step(E, F, idx, 1.0, 1.0, 1e-6)
+    e1.record()
+    torch.cuda.synchronize()
+    print(f"student training: {a.student_steps} steps of {int(idx.numel())} "
+          f"atoms, {e0.elapsed_time(e1) / a.student_steps:.3f} ms per step")
+    p.close()
 
 
 def main():

@@ -642,37 +642,6 @@ struct n2p2b_context
                     double const a = (4.0 * std::atan(1.0)) / g.rc;
                     d.a2 = a * a;
                 }
-                // Product-form runs whose etas are integer multiples m of
-                // the smallest: exp(-eta r^2) = exp(-eta_min r^2)^m, one
-                // exponential per triplet for all runs.
-                d.expChain = 0;
-                d.etaBase = 0.0;
-                if (d.shapes > 0)
-                {
-                    int const ns = d.shapes;
-                    int const runs = (int)g.members.size() / ns;
-                    double emin = el.sfs[g.members[0]].eta;
-                    for (int r = 1; r < runs; ++r)
-                        emin = std::min(emin, el.sfs[g.members[r * ns]].eta);
-                    bool ok = emin > 0.0;
-                    for (int r = 0; r < runs && ok; ++r)
-                    {
-                        double const q = el.sfs[g.members[r * ns]].eta / emin;
-                        double const m = std::round(q);
-                        ok = m >= 1.0 && m <= 1024.0
-                             && std::fabs(q - m) <= 1e-12 * m;
-                    }
-                    if (ok)
-                    {
-                        d.expChain = 1;
-                        d.etaBase = emin;
-                        for (int k = 0; k < d.mcnt; ++k)
-                        {
-                            DevMember& mm = tabMembers[d.mbeg + k];
-                            mm.etaMult = (int16_t)std::lround(mm.eta / emin);
-                        }
-                    }
-                }
                 {
                     int zmax = 0;
                     for (int mi2 : g.members)

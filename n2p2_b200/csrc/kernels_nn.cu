@@ -388,16 +388,20 @@ selfDerivativeKernel(ForceLaunch const L, T* __restrict__ out)
     }
 }
 
-// Pass 2: thread per atom.
-__global__ void gatherForceKernel(ForceLaunch const L)
+// Pass 2: warp per atom.  Lane l sums the mirror pair terms of entries
+// l, l + 32, ... of the atom in that order, then a fixed butterfly adds the
+// lanes' partial sums, so every run adds in the same order (deterministic)
+// while the 32 lanes' gathers are in flight together.
+__global__ void __launch_bounds__(256)
+gatherForceKernel(ForceLaunch const L)
 {
-    int const i = blockIdx.x * blockDim.x + threadIdx.x;
+    int const lane = threadIdx.x & 31;
+    long const i = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (i >= L.n) return;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
-    double fx = L.selfF[(long)i * 3 + 0];
-    double fy = L.selfF[(long)i * 3 + 1];
-    double fz = L.selfF[(long)i * 3 + 2];
-    for (int e = L.nbrOff[i]; e < L.nbrOff[i + 1]; ++e)
+    double fx = 0.0, fy = 0.0, fz = 0.0;
+    int const eb = L.nbrOff[i], ee = L.nbrOff[i + 1];
+    for (int e = eb + lane; e < ee; e += 32)
     {
         if (L.nbrIdx[e] == i) continue;
         long const m = L.mirror[e];
@@ -406,10 +410,21 @@ __global__ void gatherForceKernel(ForceLaunch const L)
         fy += L.pairF[m * 3 + 1];
         fz += L.pairF[m * 3 + 2];
     }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (lane != 0) return;
+    fx += L.selfF[i * 3 + 0];
+    fy += L.selfF[i * 3 + 1];
+    fz += L.selfF[i * 3 + 2];
     // Atom::toPhysicalUnits: f /= convEnergy / convLength.
-    L.F[(long)i * 3 + 0] = fx / L.forceScale;
-    L.F[(long)i * 3 + 1] = fy / L.forceScale;
-    L.F[(long)i * 3 + 2] = fz / L.forceScale;
+    L.F[i * 3 + 0] = fx / L.forceScale;
+    L.F[i * 3 + 1] = fy / L.forceScale;
+    L.F[i * 3 + 2] = fz / L.forceScale;
 }
 
 // Deterministic energy sum (fixed tree) + Structure::toPhysicalUnits +
@@ -471,38 +486,50 @@ __global__ void energyBatchKernel(BatchEnergyLaunch const L)
     }
 }
 
-__global__ void targetForceKernel(TargetForceLaunch const L)
+__global__ void __launch_bounds__(256)
+targetForceKernel(TargetForceLaunch const L)
 {
-    int const m = blockIdx.x * blockDim.x + threadIdx.x;
+    // Warp per target: lane l sums reverse entries l, l + 32, ... in that
+    // order, a fixed butterfly adds the lanes (deterministic).
+    int const lane = threadIdx.x & 31;
+    long const m = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (m >= L.numTargets) return;
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
     double fx = 0.0, fy = 0.0, fz = 0.0;
-    if (m < L.numLocal)
-    {
-        fx = L.selfF[(long)m * 3 + 0];
-        fy = L.selfF[(long)m * 3 + 1];
-        fz = L.selfF[(long)m * 3 + 2];
-    }
-    for (int k = L.revOff[m]; k < L.revOff[m + 1]; ++k)
+    for (int k = L.revOff[m] + lane; k < L.revOff[m + 1]; k += 32)
     {
         long const e = L.revEntry[k];
         fx += L.pairF[e * 3 + 0];
         fy += L.pairF[e * 3 + 1];
         fz += L.pairF[e * 3 + 2];
     }
-    L.F[(long)m * 3 + 0] = fx / L.forceScale;
-    L.F[(long)m * 3 + 1] = fy / L.forceScale;
-    L.F[(long)m * 3 + 2] = fz / L.forceScale;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+    {
+        fx += __shfl_xor_sync(0xffffffffu, fx, o);
+        fy += __shfl_xor_sync(0xffffffffu, fy, o);
+        fz += __shfl_xor_sync(0xffffffffu, fz, o);
+    }
+    if (lane != 0) return;
+    if (m < L.numLocal)
+    {
+        fx += L.selfF[m * 3 + 0];
+        fy += L.selfF[m * 3 + 1];
+        fz += L.selfF[m * 3 + 2];
+    }
+    L.F[m * 3 + 0] = fx / L.forceScale;
+    L.F[m * 3 + 1] = fy / L.forceScale;
+    L.F[m * 3 + 2] = fz / L.forceScale;
 }
 
 } // namespace
 
 void launchTargetForces(TargetForceLaunch const& L, cudaStream_t s)
 {
-    int const tb = 128;
-    int const g = (L.numTargets + tb - 1) / tb;
+    int const tb = 256;    // 8 targets (warps) per block
+    long const g = ((long)L.numTargets * 32 + tb - 1) / tb;
     noteLaunches(1);
-    targetForceKernel<<<g > 0 ? g : 1, tb, 0, s>>>(L);
+    targetForceKernel<<<g > 0 ? (int)g : 1, tb, 0, s>>>(L);
 }
 
 void launchEnergyBatch(BatchEnergyLaunch const& L, cudaStream_t s)
@@ -549,8 +576,9 @@ void launchForces(ForceLaunch const& L, cudaStream_t s)
     else
         pairForceKernel<double><<<grid > 0 ? grid : 1, 32 * warps, shm, s>>>(L);
     if (!L.gather) return;
-    int const tb = 128;
-    gatherForceKernel<<<(L.n + tb - 1) / tb > 0 ? (L.n + tb - 1) / tb : 1, tb,
+    int const tb = 256;    // 8 atoms (warps) per block
+    long const gb = ((long)L.n * 32 + tb - 1) / tb;
+    gatherForceKernel<<<gb > 0 ? (int)gb : 1, tb,
                         0, s>>>(L);
 }
 

@@ -266,23 +266,6 @@ __device__ __forceinline__ R powInt16(R x, int n)
     return result;
 }
 
-// x^m for a run multiple 1 <= m <= 1024 (exponentiation by squaring; lanes
-// of a round share m, so the loop does not diverge).
-template <typename R>
-__device__ __forceinline__ R powMult(R x, int m)
-{
-    R result = R(1);
-    unsigned k = (unsigned)m;
-    while (true)
-    {
-        if (k & 1u) result *= x;
-        k >>= 1;
-        if (k == 0u) break;
-        x *= x;
-    }
-    return result;
-}
-
 // Inverse factorials 1 / n! as compile-time constants.
 template <int N>
 struct InvFact
@@ -1226,7 +1209,6 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                     aPz[r][s] = R(0);
                 }
             R eta2[NRC], etaN[NRC];
-            int emul[NRC];
             R const* Er[NRC];
 #pragma unroll
             for (int r = 0; r < NRC; ++r)
@@ -1235,17 +1217,13 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                 DevMember const& mm = M[g.mbeg + rr * NS];
                 eta2[r] = R(2) * R(mm.eta);
                 etaN[r] = -R(mm.eta);
-                emul[r] = mm.etaMult;
                 Er[r] = W.E + (long)mm.expIdx * capE;
             }
-            // FP64: r_jk's cutoff from a power series in r_jk^2 and one
-            // exponential for all runs when their etas are integer
-            // multiples of the smallest (see cosSincSeries, DevGroup).
+            // FP64: r_jk's cosine cutoff from power series in r_jk^2 (see
+            // cosSincSeries, DevGroup::cosSeries).
             bool const series = (sizeof(R) == 8) && (CT == 1) && NARROW
                               && g.cosSeries;
-            bool const chain = (sizeof(R) == 8) && NARROW && g.expChain;
             R const a2 = R(g.a2);
-            R const etaB = -R(g.etaBase);
             if (valid && rb < nr)
             {
                 R const cr0 = invij * invij;  // 1 / r_ij^2
@@ -1326,26 +1304,11 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                             Z1[s] = zl[s] * X1;
                             Z3[s] = zl[s] * X3;
                         }
-                        // exp(-eta_r r_jk^2) per run
-                        R ejk[NRC];
-                        if (NARROW && chain)
-                        {
-                            R const b = mexp(etaB * r2);
-#pragma unroll
-                            for (int r = 0; r < NRC; ++r)
-                                ejk[r] = powMult(b, emul[r]);
-                        }
-                        else if (NARROW)
-                        {
-#pragma unroll
-                            for (int r = 0; r < NRC; ++r)
-                                ejk[r] = mexp(etaN[r] * r2);
-                        }
 #pragma unroll
                         for (int r = 0; r < NRC; ++r)
                         {
                             R vexp = Er[r][t] * Er[r][k];
-                            if (NARROW) vexp *= ejk[r];
+                            if (NARROW) vexp *= mexp(etaN[r] * r2);
                             R const e2p = eta2[r] * pfc;
                             R const Y1 = pr1 - e2p;
                             R const Y3 = NARROW ? e2p - pr3 : R(0);

@@ -39,13 +39,10 @@ struct DevGroup
     int    cosSeries;   // 1: cosine cutoff with alpha = 0, evaluated for a
                         // pair distance as power series in (pi r / rc)^2
                         // (no square root, no sin/cos)
-    int    expChain;    // product form: 1 if every eta run is an integer
-                        // multiple (DevMember::etaMult) of etaBase
     double rc, rc2;     // cutoff radius and its square
     double rci, iw;     // CutoffFunction::rci, iw  (alpha-shifted inner cutoff)
     double rcinv;       // 1 / rc
     double a2;          // (pi / rc)^2 (cosSeries)
-    double etaBase;     // smallest eta of the runs (expChain)
 };
 
 // One group member.  Angular members carry the SymGrpExpAngn::sortMembers
@@ -75,7 +72,6 @@ struct DevMember
                           // fills the atom's exp table expIdx
     int16_t slot[kMaxElem];  // dG/dr slot per neighbor element, -1 = none
     int16_t expIdx;       // per-element index of the member's (eta, rs) run
-    int16_t etaMult;      // eta / DevGroup::etaBase when expChain
 };
 
 struct SFParams
