@@ -2321,7 +2321,7 @@ struct n2p2b_context
         TuneChoice best{sfVariant, sfSortCats, nlWarpsPerBlock, t0};
         std::string rep;
         for (int v = 0; v < 4; ++v)
-            for (int so = 1; so <= 3; so += 2)
+            for (int so : {1, 3, 5, 7})
                 for (int w : nls)
                 {
                     sfVariant = v;

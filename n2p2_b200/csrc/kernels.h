@@ -129,7 +129,9 @@ struct SFLaunch
     long           warpBytes = 0;     // shared memory per warp (set by launcher)
     int            variant = 0;       // product-form shape / run chunking
     int            sortCats = 0;      // bit 0: order work categories by
-                                      // partners; bit 1: balanced owners
+                                      // partners; bit 1: balanced owners;
+                                      // bit 2: one item list of the
+                                      // segment ordered by partner count
     int const*     elem = nullptr;
     int const*     nbrOff = nullptr;
     int const*     nbrCountElem = nullptr;
@@ -152,9 +154,11 @@ int sfAtomsPerBlock();
 // Kernel variant matching the potential's product-form groups:
 // 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
 int sfDefaultVariant(SFParams const& P);
-// Default SFLaunch::sortCats: the balanced owner order (bit 1) pays for its
-// per-atom sort when an element has many angular members (long per-pair
-// work); fewer members keep positional order.
+// Default SFLaunch::sortCats: the segment-wide item order by partner count
+// (bit 2) for the product-form angular path whenever there are angular
+// members; for the general angular paths categories by partner count
+// (bit 0) and, with many angular members (long per-pair work), the
+// balanced owner order (bit 1).
 int sfDefaultSort(SFParams const& P);
 
 // Atomic neural networks (forward + dE/dG) on the SIMT cores: FP64 (plain

@@ -80,7 +80,10 @@ int sfDefaultSort(SFParams const& P)
             if (P.groups[g].type != 2) m += P.groups[g].mcnt;
         most = std::max(most, m);
     }
-    return most >= 64 ? 3 : 1;
+    // Bit 2 (the product-form path's segment-wide item order) whenever
+    // there are angular members; bits 0 and 1 serve the general paths.
+    if (most == 0) return 1;
+    return most >= 64 ? 7 : 5;
 }
 
 void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,

@@ -325,8 +325,12 @@ struct WarpMem
     unsigned* bits;   // [owner][words]
     R*        wpG;    // [maxSF]
     struct Cat*  cats;  // work-item categories of the current segment
+    unsigned*    itemList;  // sort mode 4: (category << 16 | owner) items
+    int*         itemHist;  // sort mode 4: [cap + 1] count histogram
     int          sortCats;  // bit 0: order angular categories by partner
-                            // count; bit 1: balanced owner order
+                            // count; bit 1: balanced owner order; bit 2:
+                            // one item list of the segment ordered by
+                            // partner count (buildItemList)
     // The categories are followed (kCatsBytes further on) by the balanced
     // owner order: the owners of each element ordered by their number of
     // valid partners of element e2 (descending in 32 count buckets, ties by
@@ -364,6 +368,11 @@ __device__ __forceinline__ unsigned short* ownerOrder(WarpMem<R> const& W)
         reinterpret_cast<char*>(W.cats) + kCatsBytes);
 }
 
+// Items the sort-mode-4 list holds per neighbor of the atom (a segment of
+// groups with two owner sides per group pair has up to 2 x groups x
+// neighbors items; more fall back to positional order).
+constexpr int kItemsPerCap = 4;
+
 // Bytes of one warp's shared-memory region (16-byte multiple).
 template <typename R>
 __host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap,
@@ -377,7 +386,15 @@ __host__ __device__ inline long warpBytes(int maxExp, int maxSF, int cap,
     b += kCatsBytes;                                // categories
     b += (2L * numElements * cap + 3) / 4 * 4;      // owner order
     b += 4L * 32;                                   // count buckets
+    b += 4L * kItemsPerCap * cap;                   // item list
+    b += 4L * (cap + 2);                            // its count histogram
     return (b + 15) / 16 * 16;
+}
+
+// Offset of the item list behind the categories (the layout above).
+__host__ __device__ inline long itemListOffset(int cap, int numElements)
+{
+    return kCatsBytes + (2L * numElements * cap + 3) / 4 * 4 + 4L * 32;
 }
 
 // Adds each lane's G contribution for symmetry function `sf` (-1 =
@@ -518,7 +535,123 @@ __device__ __forceinline__ Item itemOf(WarpMem<R> const& W, int ncat, int q)
 }
 
 // Partner mask of word w restricted to [pb, pe).
-__device__ __forceinline__ unsigned rangeMask(unsigned m, int w, int pb, int pe)
+__device__ __forceinline__ unsigned rangeMask(unsigned m, int w, int pb,
+                                              int pe);
+
+// Sort mode 4 (narrow angular segments): the segment's work items
+// (category, owner) as one list, ordered by the owner's number of valid
+// partners (descending; ties in item order, so the order is deterministic)
+// and, inside every round of 32, by category -- flushBySF needs the lanes
+// of a category contiguous, and a round's trip count is its largest
+// partner count, so rounds of similar counts keep the lanes busy across
+// the categories (positional or per-category order leaves about a third
+// of the lane-iterations idle on water).  Returns false when the segment
+// has more items than the list holds (the caller keeps positional order).
+template <typename R>
+__device__ bool buildItemList(WarpMem<R> const& W, int ncat, int items,
+                              int words, int cap)
+{
+    int const lane = threadIdx.x & 31;
+    if (items > kItemsPerCap * cap) return false;
+    auto itemAt = [&](int q, int& c, int& t) {
+        c = 0;
+        while (c < ncat - 1 && q >= W.cats[c].on)
+        {
+            q -= W.cats[c].on;
+            ++c;
+        }
+        t = W.cats[c].ob + q;
+    };
+    auto countOf = [&](int c, int t) {
+        Cat const& cc = W.cats[c];
+        int n = 0;
+        for (int w = cc.pb >> 5; w < (cc.pe + 31) >> 5; ++w)
+            n += __popc(rangeMask(W.bits[t * words + w], w, cc.pb, cc.pe));
+        return min(n, cap);
+    };
+    int* const hist = W.itemHist;
+    for (int k = lane; k <= cap; k += 32) hist[k] = 0;
+    __syncwarp();
+    for (int q = lane; q < items; q += 32)
+    {
+        int c, t;
+        itemAt(q, c, t);
+        atomicAdd(&hist[countOf(c, t)], 1);
+    }
+    __syncwarp();
+    if (lane == 0)
+    {
+        // hist[n] := first position of count n (descending counts).
+        int run = 0;
+        for (int k = cap; k >= 0; --k)
+        {
+            int const h = hist[k];
+            hist[k] = run;
+            run += h;
+        }
+    }
+    __syncwarp();
+    for (int q0 = 0; q0 < items; q0 += 32)
+    {
+        int const q = q0 + lane;
+        bool const act = q < items;
+        int c = 0, t = 0, n = -1 - lane;
+        if (act)
+        {
+            itemAt(q, c, t);
+            n = countOf(c, t);
+        }
+        unsigned const peers = __match_any_sync(kFull, n);
+        int const r = __popc(peers & ((1u << lane) - 1u));
+        if (act)
+            W.itemList[hist[n] + r] = ((unsigned)c << 16) | (unsigned)t;
+        __syncwarp();
+        if (act && r == 0) hist[n] += __popc(peers);
+        __syncwarp();
+    }
+    for (int q0 = 0; q0 < items; q0 += 32)
+    {
+        int const q = q0 + lane;
+        unsigned const v = q < items ? W.itemList[q] : 0xffffffffu;
+        int const key = q < items ? (int)(v >> 16) : 0x7fffffff;
+        int rank = 0;
+        for (int o = 0; o < 32; ++o)
+        {
+            int const ko = __shfl_sync(kFull, key, o);
+            rank += (ko < key || (ko == key && o < lane)) ? 1 : 0;
+        }
+        __syncwarp();
+        if (q < items) W.itemList[q0 + rank] = v;
+        __syncwarp();
+    }
+    return true;
+}
+
+template <typename R>
+__device__ __forceinline__ Item itemFromList(WarpMem<R> const& W, int items,
+                                             int q)
+{
+    Item it;
+    it.gi = -1;
+    it.key = -1;
+    it.t = 0;
+    it.et = 0;
+    it.pb = it.pe = 0;
+    if (q >= items) return it;
+    unsigned const v = W.itemList[q];
+    Cat const cc = W.cats[v >> 16];
+    it.gi = cc.gi;
+    it.key = (int)(v >> 16);
+    it.t = (int)(v & 0xffffu);
+    it.et = cc.et;
+    it.pb = cc.pb;
+    it.pe = cc.pe;
+    return it;
+}
+
+// Partner mask of word w restricted to [pb, pe).
+__device__ __forceinline__ unsigned rangeMask(unsigned m, int w, int pb,
+                                              int pe)
 {
     int const base = w << 5;
     if (base < pb) m &= kFull << (pb - base);
@@ -1163,14 +1296,19 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
-    int const items = buildCats(G, g0, g1, eb, (W.sortCats & 1) != 0,
-                                (NARROW && (W.sortCats & 2)) ? capE : 0, W,
-                                ncat);
+    bool const global = NARROW && (W.sortCats & 4);
+    int const items = buildCats(G, g0, g1, eb,
+                                (W.sortCats & 1) != 0 && !global,
+                                (NARROW && (W.sortCats & 2) && !global)
+                                    ? capE : 0,
+                                W, ncat);
+    bool const listed = global && buildItemList(W, ncat, items, words, capE);
     int maxR = 0;
     for (int gi = g0; gi < g1; ++gi) maxR = max(maxR, G[gi].mcnt / NS);
     for (int q0 = 0; q0 < items; q0 += 32)
     {
-        Item const it = itemOf(W, ncat, q0 + lane);
+        Item const it = listed ? itemFromList(W, items, q0 + lane)
+                               : itemOf(W, ncat, q0 + lane);
         bool const active = it.gi >= 0;
         DevGroup const& g = G[active ? it.gi : g0];
         int const t = it.t;
@@ -1432,6 +1570,10 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             reinterpret_cast<char*>(wbase) + off);
         long const off2 = (off + 4L * cap * words + 15) / 16 * 16;
         W.cats = reinterpret_cast<Cat*>(reinterpret_cast<char*>(wbase) + off2);
+        char* const il = reinterpret_cast<char*>(W.cats)
+                       + itemListOffset(cap, P.numElements);
+        W.itemList = reinterpret_cast<unsigned*>(il);
+        W.itemHist = reinterpret_cast<int*>(il + 4L * kItemsPerCap * cap);
     }
     W.sortCats = L.sortCats;
     R* const outG = static_cast<R*>(L.G);
