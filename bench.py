@@ -77,11 +77,11 @@ STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one FP64
 # symmetry-function launch on this workload, from the ncu capture
 # summarized in profiles/sfKernel_fp64_fp32_water12288.md (12,288-atom box,
-# 1.512 GB), scaled to the 24,576-atom frame by its neighbor entries
+# 2.090 GB), scaled to the 24,576-atom frame by its neighbor entries
 # (x 2.002).
-SF_TRAFFIC_BYTES = 3.027e9
+SF_TRAFFIC_BYTES = 4.184e9
 SF_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                     "the FP64 sfKernel on the 12,288-atom box (1.512 GB), "
+                     "the FP64 sfKernel on the 12,288-atom box (2.090 GB), "
                      "x 2.002 neighbor entries for 24,576 atoms "
                      "(profiles/sfKernel_fp64_fp32_water12288.md)")
 N_MOL = 8192
