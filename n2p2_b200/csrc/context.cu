@@ -1217,7 +1217,7 @@ struct n2p2b_context
     {
         if (sfVariant < 0)
         {
-            sfVariant = sfDefaultVariant(sfp);
+            sfVariant = sfDefaultVariant(sfp, precision);
             if (char const* v = std::getenv("N2P2B_SF_VARIANT"))
                 sfVariant = std::atoi(v);
             sfSortCats = sfDefaultSort(sfp);
@@ -2313,14 +2313,14 @@ struct n2p2b_context
         };
         if (sfVariant < 0)
         {
-            sfVariant = sfDefaultVariant(sfp);
+            sfVariant = sfDefaultVariant(sfp, precision);
             sfSortCats = sfDefaultSort(sfp);
         }
         TuneChoice const start{sfVariant, sfSortCats, nlWarpsPerBlock, 0.0};
         double const t0 = timeIt();
         TuneChoice best{sfVariant, sfSortCats, nlWarpsPerBlock, t0};
         std::string rep;
-        for (int v = 0; v < 4; ++v)
+        for (int v = 0; v < 6; ++v)
             for (int so : {1, 3, 5, 7})
                 for (int w : nls)
                 {

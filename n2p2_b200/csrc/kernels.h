@@ -152,8 +152,9 @@ std::size_t sfSharedBytes(SFParams const& P, int cap, int precision);
 int sfBlocksPerSM(SFParams const& P, int cap, int variant, int precision);
 int sfAtomsPerBlock();
 // Kernel variant matching the potential's product-form groups:
-// 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
-int sfDefaultVariant(SFParams const& P);
+// 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2);
+// 4 = (4, 3) and 5 = (8, 1) with the software-pipelined partner loop.
+int sfDefaultVariant(SFParams const& P, int precision);
 // Default SFLaunch::sortCats: the segment-wide item order by partner count
 // (bit 2) for the product-form angular path whenever there are angular
 // members; for the general angular paths categories by partner count

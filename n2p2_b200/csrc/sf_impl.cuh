@@ -91,6 +91,7 @@ constexpr int kGenericChunk = 6;
 constexpr int kCompactChunk = 8;
 constexpr unsigned kFull = 0xffffffffu;
 
+
 // Math in the compute type.  The FP32 (precision) form uses the hardware
 // approximations for exp and for the cosine cutoff's sin / cos: relative
 // errors of a few 1e-7 at the arguments met here (|x| below ~30 for exp;
@@ -1287,7 +1288,7 @@ __device__ void angularGeneric(SFParams const& P, DevGroup const* G,
 
 // Product-form angular path (see the header comment): NS shapes per eta
 // run, NRC runs per register chunk.
-template <typename R, int CT, int NS, int NRC, bool NARROW>
+template <typename R, int CT, int NS, int NRC, bool NARROW, bool PIPE>
 __device__ void angularFast(SFParams const& P, DevGroup const* G,
                             DevMember const* M, int g0, int g1,
                             int const eb[kMaxElem + 1], int cnt, int words,
@@ -1370,6 +1371,136 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                 // One loop over the lane's partners (not one per mask
                 // word): the warp's trip count is the largest partner count
                 // of its lanes, not the sum of per-word maxima.
+                if constexpr (PIPE)
+                {
+                // Software pipeline over the lane's partners: the pair part
+                // of partner n + 1 (loads, r_jk cutoff series, the runs'
+                // exponentials) is computed in the same block as the member
+                // updates of partner n, so their independent chains
+                // overlap.  The last trip computes a zero-weight copy.
+                struct PairPart
+                {
+                    R dr3[3], cost, X1, X3, pr1, pr3, pfc;
+                    R vexp[NRC];
+                };
+                auto pairPart = [&](int k, R wt) {
+                    PairPart o;
+                    R const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
+#pragma unroll
+                    for (int c = 0; c < 3; ++c) o.dr3[c] = dr2[c] - dr1[c];
+                    R const invik = W.inv[k];
+                    R const pfcik = W.fc[k] * wt;
+                    R const rinvijik = invij * invik;
+                    o.cost = (dr1[0] * dr2[0] + dr1[1] * dr2[1]
+                              + dr1[2] * dr2[2]) * rinvijik;
+                    R r2 = R(0);
+                    if (NARROW)
+                    {
+                        r2 = o.dr3[0] * o.dr3[0] + o.dr3[1] * o.dr3[1]
+                           + o.dr3[2] * o.dr3[2];
+                        R pfcjk, qjk;
+                        if (series)
+                        {
+                            double c, sc;
+                            cosSincSeries((double)(a2 * r2), c, sc);
+                            pfcjk = R(0.5) * R(c) + R(0.5);
+                            qjk = R(-0.5) * a2 * R(sc);
+                        }
+                        else
+                        {
+                            R const invjk = r2 > R(0) ? mrsqrt(r2) : R(0);
+                            R pdfcjk;
+                            cutoffFdf<R, CT>(P, g, r2 * invjk, pfcjk,
+                                             pdfcjk);
+                            qjk = pdfcjk * invjk;
+                        }
+                        o.pfc = pfcij * pfcik * pfcjk;
+                        o.pr1 = pfcik * pfcjk * pdfcrij;
+                        o.pr3 = pfcij * pfcik * qjk;
+                    }
+                    else
+                    {
+                        o.pfc = pfcij * pfcik;
+                        o.pr1 = pfcik * pdfcrij;
+                        o.pr3 = R(0);
+                    }
+                    o.X1 = o.pfc * (rinvijik - o.cost * cr0);
+                    o.X3 = o.pfc * rinvijik;
+#pragma unroll
+                    for (int r = 0; r < NRC; ++r)
+                    {
+                        R v = Er[r][t] * Er[r][k];
+                        if (NARROW) v *= mexp(etaN[r] * r2);
+                        o.vexp[r] = v;
+                    }
+                    return o;
+                };
+                auto members = [&](PairPart const& o) {
+                    R Y1[NRC], Y3[NRC];
+#pragma unroll
+                    for (int r = 0; r < NRC; ++r)
+                    {
+                        R const e2p = eta2[r] * o.pfc;
+                        Y1[r] = o.pr1 - e2p;
+                        Y3[r] = NARROW ? e2p - o.pr3 : R(0);
+                    }
+#pragma unroll
+                    for (int s = 0; s < NS; ++s)
+                    {
+                        R const pl = R(1) + lam[s] * o.cost;
+                        R const A = (pl <= R(0) || zi[s] < 1) ? R(0)
+                                  : powInt16(pl, zi[s] - 1);
+                        R const B = A * pl * o.pfc;
+                        R const Z1 = zl[s] * o.X1;
+                        R const Z3 = zl[s] * o.X3;
+#pragma unroll
+                        for (int r = 0; r < NRC; ++r)
+                        {
+                            R const wgt = o.vexp[r] * A;
+                            aG[r][s] += o.vexp[r] * B;
+                            aP1[r][s] += wgt * (Z1 + pl * Y1[r]);
+                            R const p3 = wgt * (Z3 + pl * Y3[r]);
+                            aPx[r][s] += p3 * o.dr3[0];
+                            aPy[r][s] += p3 * o.dr3[1];
+                            aPz[r][s] += p3 * o.dr3[2];
+                        }
+                    }
+                };
+                int w = wb - 1;
+                unsigned m = 0u;
+                auto next = [&]() -> int {
+                    for (;;)
+                    {
+                        while (m == 0u && ++w < we)
+                            m = rangeMask(NARROW ? W.bits[t * words + w]
+                                                 : kFull,
+                                          w, it.pb, it.pe);
+                        if (m == 0u) return -1;
+                        int const k = (w << 5) + __ffs(m) - 1;
+                        m &= m - 1;
+                        if (!NARROW && (k == t || !(W.d[k] < rc))) continue;
+                        return k;
+                    }
+                };
+                int k = next();
+                if (k >= 0)
+                {
+                    PairPart cur = pairPart(k, R(1));
+                    for (;;)
+                    {
+                        int const kn = next();
+                        bool const more = kn >= 0;
+                        PairPart const nxt = pairPart(more ? kn : k,
+                                                      more ? R(1) : R(0));
+                        members(cur);
+                        if (!more) break;
+                        cur = nxt;
+                        k = kn;
+                    }
+                }
+                }
+                else
+                {
                 int w = wb - 1;
                 unsigned m = 0u;
                 for (;;)
@@ -1464,6 +1595,7 @@ __device__ void angularFast(SFParams const& P, DevGroup const* G,
                         }
                     }
                 }
+                }
             }
 #pragma unroll
             for (int r = 0; r < NRC; ++r)
@@ -1510,7 +1642,7 @@ constexpr int kPathRadial = 1, kPathFastNarrow = 2, kPathFastWide = 4,
 
 // FP32 with up to 12 members per register chunk: at most 168 registers, so
 // that three CTAs (12 warps) fit per SM.
-template <typename R, int CT, int NS, int NRC, int PATHS>
+template <typename R, int CT, int NS, int NRC, int PATHS, bool PIPE>
 __global__ void __launch_bounds__(kThreads,
                                   (sizeof(R) == 4 && NS * NRC <= 12) ? 3 : 1)
 sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
@@ -1739,7 +1871,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             else if (fast && h.type == 3)
             {
                 if (PATHS & kPathFastNarrow)
-                    angularFast<R, CT, NS, NRC, true>(P, sG, sM, g0, g1, eb,
+                    angularFast<R, CT, NS, NRC, true, PIPE>(P, sG, sM, g0, g1, eb,
                                                       cnt, words, cap, W, out,
                                                       L.derivatives);
                 else if (lane == 0)
@@ -1748,7 +1880,7 @@ sfKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             else if (fast)
             {
                 if (PATHS & kPathFastWide)
-                    angularFast<R, CT, NS, NRC, false>(P, sG, sM, g0, g1, eb,
+                    angularFast<R, CT, NS, NRC, false, PIPE>(P, sG, sM, g0, g1, eb,
                                                        cnt, words, cap, W,
                                                        out, L.derivatives);
                 else if (lane == 0)
@@ -1835,29 +1967,29 @@ inline bool useCommonPaths(SFParams const& P, int NS)
         && L_pathsOverride() != kPathAll;
 }
 
-template <typename R, int CT, int NS, int NRC>
+template <typename R, int CT, int NS, int NRC, bool PIPE = false>
 void launchVariant(SFParams const& P, SFLaunch const& L, std::size_t shm,
                    cudaStream_t s)
 {
     if (useCommonPaths(P, NS))
     {
-        auto k = sfKernel<R, CT, NS, NRC, kPathsCommon>;
+        auto k = sfKernel<R, CT, NS, NRC, kPathsCommon, PIPE>;
         cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)shm);
         k<<<L.grid, kThreads, shm, s>>>(P, L);
         return;
     }
-    auto k = sfKernel<R, CT, NS, NRC, kPathAll>;
+    auto k = sfKernel<R, CT, NS, NRC, kPathAll, PIPE>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)shm);
     k<<<L.grid, kThreads, shm, s>>>(P, L);
 }
 
-template <typename R, int CT, int NS, int NRC>
+template <typename R, int CT, int NS, int NRC, bool PIPE = false>
 int blocksVariant(SFParams const& P, std::size_t shm)
 {
-    auto k = useCommonPaths(P, NS) ? sfKernel<R, CT, NS, NRC, kPathsCommon>
-                                   : sfKernel<R, CT, NS, NRC, kPathAll>;
+    auto k = useCommonPaths(P, NS) ? sfKernel<R, CT, NS, NRC, kPathsCommon, PIPE>
+                                   : sfKernel<R, CT, NS, NRC, kPathAll, PIPE>;
     cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
                          (int)shm);
     int blocks = 0;
@@ -1868,7 +2000,9 @@ int blocksVariant(SFParams const& P, std::size_t shm)
     return blocks;
 }
 
-// Variants: 0 = (NS 4, NRC 3), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2).
+// Variants: 0 = (NS 4, NRC 3), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2); 4 and
+// 5 = (4, 3) and (8, 1) with the partner loop software-pipelined
+// (angularFast PIPE).
 template <typename R, int CT>
 void launchForCT(SFParams const& P, SFLaunch const& L, std::size_t shm,
                  cudaStream_t s, int variant)
@@ -1878,6 +2012,8 @@ void launchForCT(SFParams const& P, SFLaunch const& L, std::size_t shm,
     case 1: launchVariant<R, CT, 4, 1>(P, L, shm, s); break;
     case 2: launchVariant<R, CT, 8, 1>(P, L, shm, s); break;
     case 3: launchVariant<R, CT, 8, 2>(P, L, shm, s); break;
+    case 4: launchVariant<R, CT, 4, 3, true>(P, L, shm, s); break;
+    case 5: launchVariant<R, CT, 8, 1, true>(P, L, shm, s); break;
     default: launchVariant<R, CT, 4, 3>(P, L, shm, s); break;
     }
 }
@@ -1890,6 +2026,8 @@ int blocksForCT(SFParams const& P, std::size_t shm, int variant)
     case 1: return blocksVariant<R, CT, 4, 1>(P, shm);
     case 2: return blocksVariant<R, CT, 8, 1>(P, shm);
     case 3: return blocksVariant<R, CT, 8, 2>(P, shm);
+    case 4: return blocksVariant<R, CT, 4, 3, true>(P, shm);
+    case 5: return blocksVariant<R, CT, 8, 1, true>(P, shm);
     default: return blocksVariant<R, CT, 4, 3>(P, shm);
     }
 }
