@@ -132,6 +132,8 @@ struct SFLaunch
                                       // partners; bit 1: balanced owners;
                                       // bit 2: one item list of the
                                       // segment ordered by partner count
+    int            recCap = 0;        // staged kernel: triplet records per
+                                      // warp batch (set by launcher)
     int const*     elem = nullptr;
     int const*     nbrOff = nullptr;
     int const*     nbrCountElem = nullptr;
@@ -150,10 +152,13 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L,
                              cudaStream_t s);
 std::size_t sfSharedBytes(SFParams const& P, int cap, int precision);
 int sfBlocksPerSM(SFParams const& P, int cap, int variant, int precision);
-int sfAtomsPerBlock();
+int sfAtomsPerBlock(SFParams const& P, int variant);
 // Kernel variant matching the potential's product-form groups:
 // 0 = (4 shapes, 3 runs per chunk), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2);
-// 4 = (4, 3) and 5 = (8, 1) with the software-pipelined partner loop.
+// 4 = (4, 3) and 5 = (8, 1) with the software-pipelined partner loop;
+// 6 = (4 shapes) and 7 = (8 shapes) staged-triplet kernel (one CTA per
+// atom, sf_staged.cuh) -- potentials it cannot serve run variant 0 / 5.
+constexpr int kSFVariants = 8;
 int sfDefaultVariant(SFParams const& P, int precision);
 // Default SFLaunch::sortCats: the segment-wide item order by partner count
 // (bit 2) for the product-form angular path whenever there are angular

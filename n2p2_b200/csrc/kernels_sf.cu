@@ -34,6 +34,44 @@ long warpBytesFor(SFParams const& P, int cap, int precision)
         : sfk::warpBytes<double>(P.maxExp, P.maxSF, cap, P.numElements);
 }
 
+bool isStaged(int variant) { return variant == 6 || variant == 7; }
+int stagedShapes(int variant) { return variant == 7 ? 8 : 4; }
+
+// The variant that runs: staged variants fall back to the per-owner kernel
+// for potentials the staged kernel does not serve.
+int effectiveVariant(SFParams const& P, int variant)
+{
+    if (isStaged(variant) && !sfk::stagedEligible(P, stagedShapes(variant)))
+        return variant == 7 ? 5 : 0;
+    return variant;
+}
+
+// Shared-memory geometry of the staged kernel.
+struct StagedGeom
+{
+    int rb = 0;
+    long warpBytes = 0;
+    std::size_t shm = 0;
+};
+
+StagedGeom stagedGeom(SFParams const& P, int cap, int precision, int ns)
+{
+    StagedGeom g;
+    if (precision != PREC_FP64)
+    {
+        g.rb = sfk::stagedRecordCap<float>(P, cap, ns);
+        g.warpBytes = sfk::stagedWarpBytes<float>(P.maxSF, ns, g.rb);
+        g.shm = sfk::stagedSharedBytes<float>(P, cap, ns, g.rb);
+    }
+    else
+    {
+        g.rb = sfk::stagedRecordCap<double>(P, cap, ns);
+        g.warpBytes = sfk::stagedWarpBytes<double>(P.maxSF, ns, g.rb);
+        g.shm = sfk::stagedSharedBytes<double>(P, cap, ns, g.rb);
+    }
+    return g;
+}
+
 } // namespace
 
 std::size_t sfSharedBytes(SFParams const& P, int cap, int precision)
@@ -42,11 +80,17 @@ std::size_t sfSharedBytes(SFParams const& P, int cap, int precision)
          + (std::size_t)sfk::kWarps * warpBytesFor(P, cap, precision);
 }
 
-int sfAtomsPerBlock() { return sfk::kWarps; }
+int sfAtomsPerBlock(SFParams const& P, int variant)
+{
+    return isStaged(effectiveVariant(P, variant)) ? 1 : sfk::kWarps;
+}
 
 int sfBlocksPerSM(SFParams const& P, int cap, int variant, int precision)
 {
-    std::size_t const shm = sfSharedBytes(P, cap, precision);
+    variant = effectiveVariant(P, variant);
+    std::size_t const shm = isStaged(variant)
+        ? stagedGeom(P, cap, precision, stagedShapes(variant)).shm
+        : sfSharedBytes(P, cap, precision);
     bool const f = precision != PREC_FP64;
     switch (P.cutoffType)
     {
@@ -94,8 +138,21 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,
                              cudaStream_t s)
 {
     SFLaunch L = L0;
-    L.warpBytes = warpBytesFor(P, L.cap, L.precision);
-    std::size_t const shm = sfSharedBytes(P, L.cap, L.precision);
+    L.variant = effectiveVariant(P, L.variant);
+    std::size_t shm;
+    if (isStaged(L.variant))
+    {
+        StagedGeom const g = stagedGeom(P, L.cap, L.precision,
+                                        stagedShapes(L.variant));
+        L.recCap = g.rb;
+        L.warpBytes = g.warpBytes;
+        shm = g.shm;
+    }
+    else
+    {
+        L.warpBytes = warpBytesFor(P, L.cap, L.precision);
+        shm = sfSharedBytes(P, L.cap, L.precision);
+    }
     noteLaunches(1);
     bool const f = L.precision != PREC_FP64;
     int const v = L.variant;

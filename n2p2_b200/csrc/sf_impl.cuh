@@ -726,19 +726,23 @@ __device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
     }
 }
 
+// Rounds of 32 owners start at qBegin and advance by qStep (several warps
+// of one atom split the owners: warp w takes qBegin = 32 w, qStep = 32 x
+// warps).
 template <typename R, int MC>
 __device__ void radialSegment(SFParams const& P, DevGroup const* G,
                               DevMember const* M, int g0, int g1,
                               int const eb[kMaxElem + 1], int cnt,
                               WarpMem<R> const& W, R* __restrict__ out,
-                              int derivatives)
+                              int derivatives, int qBegin = 0,
+                              int qStep = 32)
 {
     int const lane = threadIdx.x & 31;
     int ncat = 0;
     int const items = buildCats(G, g0, g1, eb, false, 0, W, ncat);
     int maxM = 0;
     for (int gi = g0; gi < g1; ++gi) maxM = max(maxM, G[gi].mcnt);
-    for (int q0 = 0; q0 < items; q0 += 32)
+    for (int q0 = qBegin; q0 < items; q0 += qStep)
     {
         Item const it = itemOf(W, ncat, q0 + lane);
         bool const active = it.gi >= 0;
@@ -2000,15 +2004,28 @@ int blocksVariant(SFParams const& P, std::size_t shm)
     return blocks;
 }
 
+} // namespace sfk
+} // namespace n2p2b
+
+#include "sf_staged.cuh"
+
+namespace n2p2b
+{
+namespace sfk
+{
+
 // Variants: 0 = (NS 4, NRC 3), 1 = (4, 1), 2 = (8, 1), 3 = (8, 2); 4 and
 // 5 = (4, 3) and (8, 1) with the partner loop software-pipelined
-// (angularFast PIPE).
+// (angularFast PIPE); 6 and 7 = the staged-triplet kernel for 4 and 8
+// shapes (sf_staged.cuh).
 template <typename R, int CT>
 void launchForCT(SFParams const& P, SFLaunch const& L, std::size_t shm,
                  cudaStream_t s, int variant)
 {
     switch (variant)
     {
+    case 6: launchStaged<R, CT, 4>(P, L, shm, s); break;
+    case 7: launchStaged<R, CT, 8>(P, L, shm, s); break;
     case 1: launchVariant<R, CT, 4, 1>(P, L, shm, s); break;
     case 2: launchVariant<R, CT, 8, 1>(P, L, shm, s); break;
     case 3: launchVariant<R, CT, 8, 2>(P, L, shm, s); break;
@@ -2023,6 +2040,8 @@ int blocksForCT(SFParams const& P, std::size_t shm, int variant)
 {
     switch (variant)
     {
+    case 6: return blocksStaged<R, CT, 4>(shm);
+    case 7: return blocksStaged<R, CT, 8>(shm);
     case 1: return blocksVariant<R, CT, 4, 1>(P, shm);
     case 2: return blocksVariant<R, CT, 8, 1>(P, shm);
     case 3: return blocksVariant<R, CT, 8, 2>(P, shm);

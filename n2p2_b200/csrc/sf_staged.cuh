@@ -1,0 +1,597 @@
+// Staged-triplet symmetry-function kernel for product-form narrow angular
+// groups (SymGrpExpAngn, libnnp/SymGrpExpAngn.cpp:156-403) and radial groups
+// (SymGrpExpRad, libnnp/SymGrpExpRad.cpp:144-239).  Included by
+// sf_impl.cuh, whose helpers it uses.
+//
+// Decomposition: one CTA (4 warps) per central atom i, persistent grid.  The
+// atom's neighbors are staged once per CTA (1/r, f_c, f_c'/r, the exp
+// tables) and shared by the four warps, which split the atom's work items
+// (group, owner neighbor j) round robin.  A warp runs each batch of its
+// items in two phases:
+//
+//   phase 1 (lanes over triplets): for every valid partner k of the batch's
+//     owners, the member-independent part of the triplet (j, k) is computed
+//     once and stored as a record in the warp's shared memory:
+//       v_a   = E_a(r_ij) E_a(r_ik) exp(-eta_a r_jk^2)      per eta run a
+//       beta  = A plambda pfc                                per shape s
+//       alpha'= A (zl X1 + plambda pr1) - gamma              per shape s
+//       gamma = A (zl X3 - plambda pr3)                      per shape s
+//       r_ik  (3 components)
+//     with the quantities of the product form (sf_impl.cuh: A = plambda^
+//     (zeta - 1), X1, X3, pfc, pr1, pr3);
+//   phase 2 (lanes over (member, partner slice)): lane (m, s) of member
+//     m = (run a, shape s) sums over every S-th record of the owner
+//       G  += v beta
+//       Q  += v (alpha' - 4 eta beta)        (= p1 - p3)
+//       V  += v (gamma + 2 eta beta) r_ik    (= p3 r_ik)
+//     so that the owner's slot is -(fn (Q r_ij + V)); the S partial sums of
+//     a member are added in slice order (fixed), then written once.
+//
+// Per (triplet, member) this leaves five FP64 accumulations and their
+// operands' loads; the member-independent work (r_jk's cutoff, the runs'
+// exponentials, the shape powers) is done once per ordered triplet, and no
+// lane holds more than five accumulators, so the kernel runs at four CTAs
+// (16 warps) per SM instead of the per-owner kernel's 8 warps.  All sums
+// are formed in a fixed order: results are deterministic run to run.
+#pragma once
+
+#include <algorithm>
+
+namespace n2p2b
+{
+namespace sfk
+{
+
+// Work items (owners) per batch (a batch also ends when its records fill
+// the buffer).
+constexpr int kStagedItems = 32;
+constexpr int kStagedThreads = kThreads;   // 4 warps, one atom
+constexpr int kStagedWarps = kWarps;
+// eta runs per group the records hold (groups have at most this many).
+constexpr int kStagedRuns = 4;
+// Shared memory per CTA the record capacity is sized for: four CTAs per SM.
+constexpr long kStagedTargetBytes = 56L * 1024;
+
+__host__ __device__ inline long align16(long b) { return (b + 15) / 16 * 16; }
+
+// Record of one ordered triplet (values of the compute type):
+//   [0, 3)                 r_ik
+//   [3 + 3 s, 6 + 3 s)     beta, alpha', gamma of shape s
+//   [3 + 3 NS + a]         v of eta run a
+// The stride is odd and, with 4 shapes (two partner slices read one load
+// instruction), puts the two slices' shape fields on disjoint banks.
+__host__ __device__ constexpr int stagedStride(int ns)
+{
+    return ns == 4 ? 21 : 3 + 3 * ns + kStagedRuns;
+}
+
+// Per-category constants of phase 1, shared by the warp's lanes.
+template <typename R, int NS>
+struct StagedCat
+{
+    R   lam[NS], zl[NS];
+    R   eta[kStagedRuns];
+    int zi[NS];
+    int eoff[kStagedRuns];   // offset of the run's exp table in W.E
+};
+
+// Per-warp region: G sums, categories, batch list and tables, category
+// constants, records.
+template <typename R>
+__host__ __device__ inline long stagedWarpBytes(int maxSF, int ns, int rb)
+{
+    long b = align16((long)sizeof(R) * maxSF);
+    b += kCatsBytes;
+    b += align16(4L * rb + 4L * (2 * kStagedItems + 1));
+    b += align16(ns == 4 ? (long)sizeof(StagedCat<R, 4>)
+                         : (long)sizeof(StagedCat<R, 8>));
+    b += align16((long)sizeof(R) * stagedStride(ns) * rb);
+    return b;
+}
+
+// Atom-shared region: staged neighbors and the narrow validity bits.
+template <typename R>
+__host__ __device__ inline long stagedAtomBytes(int maxExp, int cap)
+{
+    long const words = (cap + 31) / 32;
+    return align16((long)sizeof(R) * (7L + maxExp) * cap)
+         + align16(4L * cap * words);
+}
+
+template <typename R>
+__host__ __device__ inline long stagedSharedBytes(SFParams const& P, int cap,
+                                                  int ns, int rb)
+{
+    return (long)stagedTableBytes(P) + stagedAtomBytes<R>(P.maxExp, cap)
+         + kStagedWarps * stagedWarpBytes<R>(P.maxSF, ns, rb);
+}
+
+// The staged kernel serves potentials whose groups are radial or
+// product-form narrow angular with ns shapes, at most kStagedRuns eta runs
+// and at most 32 members (one lane each).
+inline bool stagedEligible(SFParams const& P, int ns)
+{
+    if ((pathsNeeded(P, ns) & ~(kPathRadial | kPathFastNarrow)) != 0)
+        return false;
+    if (!P.stageTables) return false;
+    for (int g = 0; g < P.groupBeg[P.numElements]; ++g)
+    {
+        DevGroup const& h = P.groups[g];
+        if (h.type == 3
+            && (h.shapes != ns || h.mcnt > 32 || h.mcnt % ns
+                || h.mcnt / ns > kStagedRuns))
+            return false;
+    }
+    return true;
+}
+
+// Record capacity: the largest multiple of 16 in [32, 96] whose CTA fits
+// kStagedTargetBytes (32 when none does).
+template <typename R>
+inline int stagedRecordCap(SFParams const& P, int cap, int ns)
+{
+    for (int rb = 96; rb > 32; rb -= 16)
+        if (stagedSharedBytes<R>(P, cap, ns, rb) <= kStagedTargetBytes)
+            return rb;
+    return 32;
+}
+
+// Phase 1: the record of ordered triplet (owner t, partner k) of a group
+// with constants C.
+template <typename R, int CT, int NS>
+__device__ __forceinline__ void stagedRecord(SFParams const& P,
+                                             DevGroup const& g,
+                                             StagedCat<R, NS> const& C,
+                                             int nr, bool series, bool pow16,
+                                             int t, int k,
+                                             WarpMem<R> const& W,
+                                             R* __restrict__ rec)
+{
+    R const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+    R const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
+    R const invij = W.inv[t];
+    R const pfcij = W.fc[t];
+    R const pfcik = W.fc[k];
+    R const pdfcrij = W.dfcr[t];
+    R const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1], dr2[2] - dr1[2]};
+    R const rinvijik = invij * W.inv[k];
+    R const cost = (dr1[0] * dr2[0] + dr1[1] * dr2[1] + dr1[2] * dr2[2])
+                 * rinvijik;
+    R const r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1] + dr3[2] * dr3[2];
+    // f_c(r_jk) and f_c'(r_jk) / r_jk (FP64 cosine cutoff: power series in
+    // r_jk^2, see cosSincSeries).
+    R pfcjk, qjk;
+    if ((sizeof(R) == 8) && (CT == 1) && series)
+    {
+        double c, sc;
+        cosSincSeries((double)(R(g.a2) * r2), c, sc);
+        pfcjk = R(0.5) * R(c) + R(0.5);
+        qjk = R(-0.5) * R(g.a2) * R(sc);
+    }
+    else
+    {
+        R const invjk = mrsqrt(r2);
+        R pdfcjk;
+        cutoffFdf<R, CT>(P, g, r2 * invjk, pfcjk, pdfcjk);
+        qjk = pdfcjk * invjk;
+    }
+    R const pfc = pfcij * pfcik * pfcjk;
+    R const pr1 = pfcik * pfcjk * pdfcrij;
+    R const pr3 = pfcij * pfcik * qjk;
+    R const X1 = pfc * (rinvijik - cost * (invij * invij));
+    R const X3 = pfc * rinvijik;
+    rec[0] = dr2[0];
+    rec[1] = dr2[1];
+    rec[2] = dr2[2];
+#pragma unroll
+    for (int s = 0; s < NS; ++s)
+    {
+        int const zi = C.zi[s];
+        R const pl = R(1) + C.lam[s] * cost;
+        R const A = (pl <= R(0)) ? R(0)
+                  : (pow16 && zi >= 1) ? powInt16(pl, zi - 1)
+                                       : powInt(pl, zi - 1);
+        R const D = A * pl;
+        R const Azl = A * C.zl[s];
+        R const ga = Azl * X3 - D * pr3;
+        rec[3 + 3 * s] = D * pfc;
+        rec[4 + 3 * s] = (Azl * X1 + D * pr1) - ga;
+        rec[5 + 3 * s] = ga;
+    }
+#pragma unroll
+    for (int a = 0; a < kStagedRuns; ++a)
+        if (a < nr)
+        {
+            R const* E = W.E + C.eoff[a];
+            rec[3 + 3 * NS + a] = E[t] * E[k] * mexp(-C.eta[a] * r2);
+        }
+}
+
+// A product-form narrow angular segment [g0, g1).  Categories (group, owner
+// element) are walked in order; warp w takes owners w, w + warps, ... of
+// each, in batches of owners whose partners fill at most rb records.
+template <typename R, int CT, int NS>
+__device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
+                             DevMember const* M, int g0, int g1,
+                             int const eb[kMaxElem + 1], int cnt, int words,
+                             int capE, WarpMem<R> const& W, int* list,
+                             int* bT, int* bOff, StagedCat<R, NS>* cp,
+                             R* recs, int rb, int warp, int warps,
+                             R* __restrict__ out, int derivatives)
+{
+    constexpr int NF = stagedStride(NS);
+    int const lane = threadIdx.x & 31;
+    unsigned const below = (1u << lane) - 1u;
+    int ncat = 0;
+    buildCats(G, g0, g1, eb, false, 0, W, ncat);
+    for (int c = 0; c < ncat; ++c)
+    {
+        Cat const cc = W.cats[c];
+        DevGroup const& g = G[cc.gi];
+        // Owners beyond the group's cutoff have no triplets; their slots
+        // are written as zero like the others'.
+        R const rc = R(g.rc);
+        int const mc = g.mcnt;
+        int const nr = mc / NS;
+        bool const series = g.cosSeries != 0;
+        bool const pow16 = g.powBits <= 4;
+        if (lane == 0)
+        {
+            for (int s = 0; s < NS; ++s)
+            {
+                DevMember const& mm = M[g.mbeg + s];
+                cp->lam[s] = R(mm.lambda);
+                cp->zl[s] = R(mm.zetaLambda);
+                cp->zi[s] = mm.zetaInt;
+            }
+            for (int a = 0; a < kStagedRuns; ++a)
+            {
+                DevMember const& mm = M[g.mbeg + min(a, nr - 1) * NS];
+                cp->eta[a] = R(mm.eta);
+                cp->eoff[a] = mm.expIdx * capE;
+            }
+        }
+        // Phase-2 lane: member m of slice s (S slices of the partners).
+        int const S = 32 / mc;
+        int const s = lane / mc;
+        int const m = lane - s * mc;
+        bool const p2 = s < S;
+        int const a = m / NS;
+        int const sh = m - a * NS;
+        DevMember const& lm = M[g.mbeg + (p2 ? m : 0)];
+        R const eta = R(M[g.mbeg + a * NS].eta);
+        R const eta2 = R(2) * eta, eta4 = R(4) * eta;
+        R const fn = R(lm.factorNorm);
+        R* const outL = out + (long)lm.slot[cc.et] * 3 * cnt;
+        R* const gL = W.wpG + lm.sf;
+        int const offS = 3 + 3 * sh;
+        int const offV = 3 + 3 * NS + a;
+        __syncwarp();
+        StagedCat<R, NS> const& C = *cp;
+
+        // Sums of the open owner (carried across batches when its partners
+        // span more than one).
+        R aG = R(0), aQ = R(0), aX = R(0), aY = R(0), aZ = R(0);
+        int o = warp;
+        int wcur = -1;   // word to resume the open owner at
+        while (o < cc.on)
+        {
+            // ---- phase 0: the batch's partner list, whole mask words ----
+            int n = 0, nb = 0;
+            bool open = false;
+            while (o < cc.on && nb < kStagedItems)
+            {
+                int const t = cc.ob + o;
+                int w = (wcur >= 0) ? wcur : (cc.pb >> 5);
+                int const we = (W.d[t] < rc) ? (cc.pe + 31) >> 5 : w;
+                if (lane == 0)
+                {
+                    bT[nb] = t;
+                    bOff[nb] = n;
+                }
+                for (; w < we; ++w)
+                {
+                    unsigned const mk = rangeMask(W.bits[t * words + w], w,
+                                                  cc.pb, cc.pe);
+                    int const cw = __popc(mk);
+                    if (n + cw > rb) break;
+                    if ((mk >> lane) & 1u)
+                        list[n + __popc(mk & below)] = (nb << 16)
+                                                     | ((w << 5) + lane);
+                    n += cw;
+                }
+                ++nb;
+                if (w < we)
+                {
+                    wcur = w;
+                    open = true;
+                    break;
+                }
+                wcur = -1;
+                o += warps;
+            }
+            if (lane == 0) bOff[nb] = n;
+            __syncwarp();
+            // ---- phase 1: one record per ordered triplet --------------
+            for (int r = lane; r < n; r += 32)
+            {
+                int const e = list[r];
+                stagedRecord<R, CT, NS>(P, g, C, nr, series, pow16,
+                                        bT[e >> 16], e & 0xffff, W,
+                                        recs + (long)r * NF);
+            }
+            __syncwarp();
+            // ---- phase 2: lanes (member, slice) over each owner ---------
+            for (int b = 0; b < nb; ++b)
+            {
+                int const ro = bOff[b], re = bOff[b + 1];
+                if (p2)
+                {
+                    R const* q = recs + (long)(ro + s) * NF;
+#pragma unroll 2
+                    for (int r = ro + s; r < re; r += S, q += S * NF)
+                    {
+                        R const v = q[offV];
+                        R const be = q[offS];
+                        aG += v * be;
+                        aQ += v * (q[offS + 1] - eta4 * be);
+                        R const p3 = v * (q[offS + 2] + eta2 * be);
+                        aX += p3 * q[0];
+                        aY += p3 * q[1];
+                        aZ += p3 * q[2];
+                    }
+                }
+                if (b < nb - 1 || !open)
+                {
+                    // The owner ends here: slice sums in slice order, then
+                    // the member's slot and value.
+                    for (int s2 = 1; s2 < S; ++s2)
+                    {
+                        int const src = (lane + s2 * mc) & 31;
+                        aG += __shfl_sync(kFull, aG, src);
+                        aQ += __shfl_sync(kFull, aQ, src);
+                        aX += __shfl_sync(kFull, aX, src);
+                        aY += __shfl_sync(kFull, aY, src);
+                        aZ += __shfl_sync(kFull, aZ, src);
+                    }
+                    if (lane < mc)
+                    {
+                        int const t = bT[b];
+                        if (derivatives)
+                        {
+                            outL[t] = -(fn * (aQ * W.dx[t] + aX));
+                            outL[cnt + t] = -(fn * (aQ * W.dy[t] + aY));
+                            outL[2 * cnt + t] = -(fn * (aQ * W.dz[t] + aZ));
+                        }
+                        *gL += R(0.5) * aG;
+                    }
+                    aG = aQ = aX = aY = aZ = R(0);
+                }
+            }
+            __syncwarp();
+        }
+    }
+}
+
+template <typename R, int CT, int NS>
+__global__ void __launch_bounds__(kStagedThreads, 4)
+sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
+{
+    extern __shared__ double smem0[];
+    int const ng = P.numGroups;
+    int const nm = P.numMembers;
+    int const tid = threadIdx.x;
+    DevGroup* tg = reinterpret_cast<DevGroup*>(smem0);
+    DevMember* tm = reinterpret_cast<DevMember*>(tg + ng);
+    {
+        int const* src = reinterpret_cast<int const*>(P.dGroups);
+        int* dst = reinterpret_cast<int*>(tg);
+        int const words = (int)(ng * sizeof(DevGroup) / sizeof(int));
+        for (int k = tid; k < words; k += kStagedThreads) dst[k] = src[k];
+        src = reinterpret_cast<int const*>(P.dMembers);
+        dst = reinterpret_cast<int*>(tm);
+        int const wm = (int)(nm * sizeof(DevMember) / sizeof(int));
+        for (int k = tid; k < wm; k += kStagedThreads) dst[k] = src[k];
+    }
+    DevGroup const* const sG = tg;
+    DevMember const* const sM = tm;
+    __syncthreads();
+    if (L.status[ST_FLAGS] & FLAG_ABORT) return;
+
+    int const lane = tid & 31;
+    int const warp = tid >> 5;
+    int const cap = L.cap;
+    int const words = (cap + 31) >> 5;
+    int const maxSF = P.maxSF;
+    char* const base = reinterpret_cast<char*>(smem0) + tableBytes(ng, nm);
+    R* const st = reinterpret_cast<R*>(base);
+    WarpMem<R> W;
+    W.dx = st;
+    W.dy = W.dx + cap;
+    W.dz = W.dy + cap;
+    W.d = W.dz + cap;
+    W.inv = W.d + cap;
+    W.fc = W.inv + cap;
+    W.dfcr = W.fc + cap;
+    W.E = W.dfcr + cap;
+    W.bits = reinterpret_cast<unsigned*>(
+        base + align16((long)sizeof(R) * (7L + P.maxExp) * cap));
+    char* const warps0 = base + stagedAtomBytes<R>(P.maxExp, cap);
+    char* const wp = warps0 + (long)warp * L.warpBytes;
+    W.wpG = reinterpret_cast<R*>(wp);
+    W.cats = reinterpret_cast<Cat*>(wp + align16((long)sizeof(R) * maxSF));
+    W.itemList = nullptr;
+    W.itemHist = nullptr;
+    W.sortCats = 0;
+    int const rb = L.recCap;
+    int* const list = reinterpret_cast<int*>(reinterpret_cast<char*>(W.cats)
+                                             + kCatsBytes);
+    int* const bT = list + rb;
+    int* const bOff = bT + kStagedItems;
+    char* const cpp = reinterpret_cast<char*>(list)
+                    + align16(4L * rb + 4L * (2 * kStagedItems + 1));
+    StagedCat<R, NS>* const cp = reinterpret_cast<StagedCat<R, NS>*>(cpp);
+    R* const recs = reinterpret_cast<R*>(
+        cpp + align16((long)sizeof(StagedCat<R, NS>)));
+    R* const outG = static_cast<R*>(L.G);
+    R* const outNbr = static_cast<R*>(L.dGdr);
+    int const numElements = P.numElements;
+
+    for (int i = blockIdx.x; i < L.n; i += gridDim.x)
+    {
+        int const ec = L.elem[i];
+        long const beg = L.nbrOff[i];
+        int const cnt = L.nbrOff[i + 1] - (int)beg;
+        if (cnt > cap)
+        {
+            if (tid == 0)
+            {
+                atomicOr(&L.status[ST_FLAGS], FLAG_SF_CAPACITY);
+                atomicCAS(&L.status[ST_BAD_ATOM], -1, i);
+            }
+            continue;
+        }
+        int eb[kMaxElem + 1];
+        eb[0] = 0;
+        for (int e = 0; e < numElements; ++e)
+            eb[e + 1] = eb[e] + L.nbrCountElem[(long)i * numElements + e];
+        for (int e = numElements + 1; e <= kMaxElem; ++e) eb[e] = eb[numElements];
+        for (int t = tid; t < cnt; t += kStagedThreads)
+        {
+            double const dd = L.dd[beg + t];
+            W.dx[t] = R(L.dx[beg + t]);
+            W.dy[t] = R(L.dy[beg + t]);
+            W.dz[t] = R(L.dz[beg + t]);
+            W.d[t] = R(dd);
+            W.inv[t] = R(1.0 / dd);
+        }
+        for (int k = lane; k < maxSF; k += 32) W.wpG[k] = R(0);
+        __syncthreads();
+        R* out = outNbr + beg * (long)P.maxSlots * 3;
+        double fcRc = -1.0;
+        double bitsRc = -1.0;
+        int const gb = P.groupBeg[ec], ge = P.groupBeg[ec + 1];
+        int g0 = gb;
+        while (g0 < ge)
+        {
+            DevGroup const& h = sG[g0];
+            int g1 = g0 + 1;
+            while (g1 < ge && sG[g1].type == h.type && sG[g1].rc == h.rc
+                   && g1 - g0 < segCap(h.type))
+                ++g1;
+            if (h.rc != fcRc)
+            {
+                for (int t = tid; t < cnt; t += kStagedThreads)
+                {
+                    R fc, dfc;
+                    cutoffFdf<R, CT>(P, h, W.d[t], fc, dfc);
+                    W.fc[t] = fc;
+                    W.dfcr[t] = dfc * W.inv[t];
+                }
+                fcRc = h.rc;
+            }
+            if (h.type == 3 && h.rc != bitsRc)
+            {
+                // Narrow-angular validity: k != t, r_ik < rc, r_jk^2 < rc^2.
+                R const rc = R(h.rc), rc2 = R(h.rc2);
+                for (int t = tid; t < cnt; t += kStagedThreads)
+                {
+                    R const x = W.dx[t], y = W.dy[t], z = W.dz[t];
+                    for (int w = 0; w < words; ++w)
+                    {
+                        unsigned m = 0u;
+                        int const kb = w << 5;
+                        int const ke = min(cnt, kb + 32);
+                        for (int k = kb; k < ke; ++k)
+                        {
+                            R const a = W.dx[k] - x;
+                            R const b = W.dy[k] - y;
+                            R const c = W.dz[k] - z;
+                            bool const ok = (k != t) && (W.d[k] < rc)
+                                          && (a * a + b * b + c * c < rc2);
+                            m |= (ok ? 1u : 0u) << (k - kb);
+                        }
+                        W.bits[t * words + w] = m;
+                    }
+                }
+                bitsRc = h.rc;
+            }
+            if (h.type == 3)
+            {
+                // E(r) = exp(-eta (r - rs)^2) per distinct (eta, rs) of the
+                // element.
+                for (int gi = g0; gi < g1; ++gi)
+                {
+                    DevGroup const& g = sG[gi];
+                    for (int l = 0; l < g.mcnt; ++l)
+                    {
+                        DevMember const& mm = sM[g.mbeg + l];
+                        if (!mm.fillExp) continue;
+                        R* E = W.E + (long)mm.expIdx * cap;
+                        R const eta = R(mm.eta), rs = R(mm.rs);
+                        for (int t = tid; t < cnt; t += kStagedThreads)
+                        {
+                            R const rr = W.d[t] - rs;
+                            E[t] = mexp(-eta * rr * rr);
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+            if (h.type == 2 || h.type == 12)
+                radialSegment<R, kGenericChunk>(P, sG, sM, g0, g1, eb, cnt, W,
+                                                out, L.derivatives, 32 * warp,
+                                                32 * kStagedWarps);
+            else if (h.type == 3 && h.shapes == NS)
+                stagedNarrow<R, CT, NS>(P, sG, sM, g0, g1, eb, cnt, words, cap,
+                                        W, list, bT, bOff, cp, recs, rb, warp,
+                                        kStagedWarps, out, L.derivatives);
+            else if (tid == 0)
+                atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
+            __syncthreads();
+            g0 = g1;
+        }
+        // G: the warps' sums in warp order, then the scaling transform.
+        int const nsf = P.numSF[ec];
+        SFScale const* sc = L.scale + (long)ec * maxSF;
+        for (int s = tid; s < nsf; s += kStagedThreads)
+        {
+            R v = R(0);
+            for (int w = 0; w < kStagedWarps; ++w)
+                v += reinterpret_cast<R const*>(warps0 + (long)w
+                                                * L.warpBytes)[s];
+            SFScale const q = sc[s];
+            outG[(long)i * maxSF + s] =
+                R(q.smin + q.b * (q.q * (double)v - q.shift));
+        }
+        __syncthreads();
+    }
+}
+
+template <typename R, int CT, int NS>
+void launchStaged(SFParams const& P, SFLaunch const& L, std::size_t shm,
+                  cudaStream_t s)
+{
+    auto k = sfStagedKernel<R, CT, NS>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)shm);
+    k<<<L.grid, kStagedThreads, shm, s>>>(P, L);
+}
+
+template <typename R, int CT, int NS>
+int blocksStaged(std::size_t shm)
+{
+    auto k = sfStagedKernel<R, CT, NS>;
+    cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (int)shm);
+    int blocks = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, k,
+                                                      kStagedThreads, shm)
+            != cudaSuccess
+        || blocks < 1)
+        blocks = 1;
+    return blocks;
+}
+
+} // namespace sfk
+} // namespace n2p2b
