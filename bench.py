@@ -75,15 +75,30 @@ POT = os.path.join(POT_DIR, "h2o_52")
 STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
           "forces")
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one FP64
-# symmetry-function launch on this workload, from the ncu capture
-# summarized in profiles/sfKernel_fp64_fp32_water12288.md (12,288-atom box,
-# 2.090 GB), scaled to the 24,576-atom frame by its neighbor entries
-# (x 2.002).
-SF_TRAFFIC_BYTES = 4.184e9
-SF_TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of "
-                     "the FP64 sfKernel on the 12,288-atom box (2.090 GB), "
-                     "x 2.002 neighbor entries for 24,576 atoms "
-                     "(profiles/sfKernel_fp64_fp32_water12288.md)")
+# symmetry-function launch on this workload, per kernel family, from the
+# ncu captures summarized under profiles/ (12,288-atom box), scaled to the
+# 24,576-atom frame by its neighbor entries (x 2.002): the staged-triplet
+# kernel (variants 6, 7; the default) and the per-owner kernel (0-5).
+SF_TRAFFIC = {
+    "staged": (2.255e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                        "the FP64 sfStagedKernel on the 12,288-atom box "
+                        "(1.126 GB), x 2.002 neighbor entries for 24,576 "
+                        "atoms (profiles/sfStagedKernel_fp64_fp32_"
+                        "water12288.md)"),
+    "owner": (4.184e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+                       "the FP64 per-owner sfKernel on the 12,288-atom box "
+                       "(2.090 GB), x 2.002 neighbor entries for 24,576 "
+                       "atoms (profiles/sfKernel_fp64_fp32_water12288.md)"),
+}
+
+
+def sf_family(tune: str) -> str:
+    """Kernel family of the autotuner's choice ("... sf variant N ...")."""
+    import re
+    m = re.search(r"sf variant (\d+)", tune or "")
+    return "staged" if m and int(m.group(1)) >= 6 else "owner"
+
+
 N_MOL = 8192
 SEED = 2026
 N_FRAMES = 100
@@ -859,7 +874,9 @@ def run_ours(a):
         "stage_ms_per_step": dict(zip(STAGES, per)),
         "autotune": tune,
         "roofline": {
-            "kernel": "sfKernel<double> (symmetry functions + dG/dr)",
+            "kernel": ("sfStagedKernel<double>" if sf_family(tune) == "staged"
+                       else "sfKernel<double>")
+                      + " (symmetry functions + dG/dr)",
             "bound": "fp64",
             "achieved": sf_tflops, "peak": fp64_peak, "unit": "TFLOP/s",
             "frac": sf_tflops / fp64_peak,
@@ -870,8 +887,8 @@ def run_ours(a):
                                "triplet and neighbor counts, see work) / "
                                "the SF stage's CUDA-event time",
             "algorithmic_flops_per_launch": wm["flops_sf"],
-            "traffic": SF_TRAFFIC_BYTES,
-            "traffic_source": SF_TRAFFIC_SOURCE,
+            "traffic": SF_TRAFFIC[sf_family(tune)][0],
+            "traffic_source": SF_TRAFFIC[sf_family(tune)][1],
             "hbm": {"achieved": gbs, "peak": hbm_peak, "unit": "GB/s",
                     "frac": gbs / hbm_peak,
                     "peak_source": f"{peak_kind} (MEASURED_PEAKS.json "
