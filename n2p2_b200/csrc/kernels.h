@@ -134,6 +134,8 @@ struct SFLaunch
                                       // segment ordered by partner count
     int            recCap = 0;        // staged kernel: triplet records per
                                       // warp batch (set by launcher)
+    int            tablesShared = 0;  // staged kernel: group / member
+                                      // tables staged in shared memory
     int const*     elem = nullptr;
     int const*     nbrOff = nullptr;
     int const*     nbrCountElem = nullptr;

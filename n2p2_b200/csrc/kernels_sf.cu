@@ -50,26 +50,26 @@ int effectiveVariant(SFParams const& P, int variant)
 struct StagedGeom
 {
     int rb = 0;
+    bool tables = false;
     long warpBytes = 0;
     std::size_t shm = 0;
 };
 
-StagedGeom stagedGeom(SFParams const& P, int cap, int precision, int ns)
+template <typename R>
+StagedGeom stagedGeomT(SFParams const& P, int cap, int ns)
 {
     StagedGeom g;
-    if (precision != PREC_FP64)
-    {
-        g.rb = sfk::stagedRecordCap<float>(P, cap, ns);
-        g.warpBytes = sfk::stagedWarpBytes<float>(P.maxSF, ns, g.rb);
-        g.shm = sfk::stagedSharedBytes<float>(P, cap, ns, g.rb);
-    }
-    else
-    {
-        g.rb = sfk::stagedRecordCap<double>(P, cap, ns);
-        g.warpBytes = sfk::stagedWarpBytes<double>(P.maxSF, ns, g.rb);
-        g.shm = sfk::stagedSharedBytes<double>(P, cap, ns, g.rb);
-    }
+    g.tables = sfk::stagedTablesShared<R>(P, cap, ns);
+    g.rb = sfk::stagedRecordCap<R>(P, cap, ns, g.tables);
+    g.warpBytes = sfk::stagedWarpBytes<R>(P.maxSF, ns, g.rb);
+    g.shm = sfk::stagedSharedBytes<R>(P, cap, ns, g.rb, g.tables);
     return g;
+}
+
+StagedGeom stagedGeom(SFParams const& P, int cap, int precision, int ns)
+{
+    return precision != PREC_FP64 ? stagedGeomT<float>(P, cap, ns)
+                                  : stagedGeomT<double>(P, cap, ns);
 }
 
 } // namespace
@@ -147,6 +147,7 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,
         StagedGeom const g = stagedGeom(P, L.cap, L.precision,
                                         stagedShapes(L.variant));
         L.recCap = g.rb;
+        L.tablesShared = g.tables ? 1 : 0;
         L.warpBytes = g.warpBytes;
         shm = g.shm;
     }

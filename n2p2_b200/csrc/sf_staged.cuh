@@ -98,11 +98,14 @@ __host__ __device__ inline long stagedAtomBytes(int maxExp, int cap)
          + align16(4L * cap * words);
 }
 
+// tables: the group and member tables are staged in shared memory (else
+// read from global memory through L1).
 template <typename R>
 __host__ __device__ inline long stagedSharedBytes(SFParams const& P, int cap,
-                                                  int ns, int rb)
+                                                  int ns, int rb, bool tables)
 {
-    return (long)stagedTableBytes(P) + stagedAtomBytes<R>(P.maxExp, cap)
+    return (tables ? (long)stagedTableBytes(P) : 0L)
+         + stagedAtomBytes<R>(P.maxExp, cap)
          + kStagedWarps * stagedWarpBytes<R>(P.maxSF, ns, rb);
 }
 
@@ -113,7 +116,6 @@ inline bool stagedEligible(SFParams const& P, int ns)
 {
     if ((pathsNeeded(P, ns) & ~(kPathRadial | kPathFastNarrow)) != 0)
         return false;
-    if (!P.stageTables) return false;
     for (int g = 0; g < P.groupBeg[P.numElements]; ++g)
     {
         DevGroup const& h = P.groups[g];
@@ -128,12 +130,23 @@ inline bool stagedEligible(SFParams const& P, int ns)
 // Record capacity: the largest multiple of 16 in [32, 96] whose CTA fits
 // kStagedTargetBytes (32 when none does).
 template <typename R>
-inline int stagedRecordCap(SFParams const& P, int cap, int ns)
+inline int stagedRecordCap(SFParams const& P, int cap, int ns, bool tables)
 {
     for (int rb = 96; rb > 32; rb -= 16)
-        if (stagedSharedBytes<R>(P, cap, ns, rb) <= kStagedTargetBytes)
+        if (stagedSharedBytes<R>(P, cap, ns, rb, tables) <= kStagedTargetBytes)
             return rb;
     return 32;
+}
+
+// The tables are staged in shared memory when the CTA fits
+// kStagedTargetBytes with the smallest record capacity; larger tables (the
+// 92-SF potential's) are read from global memory, which keeps four CTAs
+// per SM.
+template <typename R>
+inline bool stagedTablesShared(SFParams const& P, int cap, int ns)
+{
+    return P.stageTables
+        && stagedSharedBytes<R>(P, cap, ns, 32, true) <= kStagedTargetBytes;
 }
 
 // Phase 1: the record of ordered triplet (owner t, partner k) of a group
@@ -381,9 +394,15 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     int const ng = P.numGroups;
     int const nm = P.numMembers;
     int const tid = threadIdx.x;
-    DevGroup* tg = reinterpret_cast<DevGroup*>(smem0);
-    DevMember* tm = reinterpret_cast<DevMember*>(tg + ng);
+    // Group and member tables: staged in shared memory when they fit the
+    // CTA's budget, else read from global memory through L1.
+    bool const tables = L.tablesShared != 0;
+    DevGroup const* sG = P.dGroups;
+    DevMember const* sM = P.dMembers;
+    if (tables)
     {
+        DevGroup* tg = reinterpret_cast<DevGroup*>(smem0);
+        DevMember* tm = reinterpret_cast<DevMember*>(tg + ng);
         int const* src = reinterpret_cast<int const*>(P.dGroups);
         int* dst = reinterpret_cast<int*>(tg);
         int const words = (int)(ng * sizeof(DevGroup) / sizeof(int));
@@ -392,9 +411,9 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
         dst = reinterpret_cast<int*>(tm);
         int const wm = (int)(nm * sizeof(DevMember) / sizeof(int));
         for (int k = tid; k < wm; k += kStagedThreads) dst[k] = src[k];
+        sG = tg;
+        sM = tm;
     }
-    DevGroup const* const sG = tg;
-    DevMember const* const sM = tm;
     __syncthreads();
     if (L.status[ST_FLAGS] & FLAG_ABORT) return;
 
@@ -403,7 +422,8 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     int const cap = L.cap;
     int const words = (cap + 31) >> 5;
     int const maxSF = P.maxSF;
-    char* const base = reinterpret_cast<char*>(smem0) + tableBytes(ng, nm);
+    char* const base = reinterpret_cast<char*>(smem0)
+                     + (tables ? tableBytes(ng, nm) : 0);
     R* const st = reinterpret_cast<R*>(base);
     WarpMem<R> W;
     W.dx = st;
