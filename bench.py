@@ -539,8 +539,10 @@ def measure_forms(box, frames, elem, dev_frames, stream, lib, steps, local):
         "mixed": "FP32 symmetry functions + dG/dr; NN on tcgen05 with BF16 "
                  "hi/lo operand pairs (3 MMAs per step), FP32 accumulation; "
                  "FP64 displacements, energy sum, force accumulation",
-        "bf16": "as mixed with single BF16 operands (1 MMA per step); "
-                "meets_targets says whether its RMSE is inside the targets",
+        "bf16": "as mixed, except single BF16 deltas against hi/lo "
+                "weights in the backward GEMMs of the hidden layers above "
+                "the first (2 MMAs per step there); meets_targets says "
+                "whether its RMSE is inside the targets",
         "student_gated": "FP32 symmetry functions; distilled 92-32-1 FP32 "
                          "student for atoms inside its training range, the "
                          "mixed-precision teacher for the others",

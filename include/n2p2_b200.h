@@ -71,7 +71,12 @@ int         n2p2b_set_stream(n2p2b_context* ctx, void* stream);
  * neighbor displacements, the energy sum and the force accumulation stay
  * FP64.  N2P2B_PRECISION_MIXED splits each NN operand into BF16 high and low
  * parts (three tensor-core products per step, about 16 significant bits);
- * N2P2B_PRECISION_BF16 uses single BF16 operands (8 significant bits).
+ * N2P2B_PRECISION_BF16 splits the operands of the forward sweep and of
+ * dE/dG as MIXED does and keeps the back-propagated derivatives of the
+ * hidden layers above the first in single BF16 (8 significant bits) against
+ * split weights (two products per step): roundings there perturb each
+ * atom's forces independently, while rounded weights or activations of the
+ * forward sweep bias every atom's energy alike.
  * Getters return the FP32 intermediates widened to double.  Returns
  * N2P2B_ERR_SETUP if the potential's networks do not fit the tensor-core
  * kernel (more than one output, a layer wider than 256). */

@@ -200,7 +200,9 @@ struct n2p2b_context
     int          maxSlots = 0;
     DevBuf       sfScale, nnW, slotSF;
     // Mixed forms (FP32 symmetry functions, BF16 tensor-core NNs); index 0
-    // = single BF16 operands (PREC_BF16), 1 = hi/lo split (PREC_MIXED).
+    // = PREC_BF16 (hi/lo operands in the forward sweep and for dE/dG, single
+    // BF16 deltas with hi/lo weights in the other backward GEMMs: 2 MMAs per
+    // K-step there), 1 = PREC_MIXED (hi/lo operands everywhere: 3 MMAs).
     int          precision = PREC_FP64;
     TcNNParams   tcp[2] = {};
     bool         tcOk[2] = {false, false};
@@ -674,8 +676,8 @@ struct n2p2b_context
         std::vector<unsigned char> tcWeights[2];
         std::vector<float> tcFloats[2];
         for (int k = 0; k < 2; ++k)
-            tcOk[k] = tcBuild(nnp, blob, k, tcp[k], tcWeights[k], tcFloats[k],
-                              tcWhy[k]);
+            tcOk[k] = tcBuild(nnp, blob, k == 1 ? 1 : 2, tcp[k], tcWeights[k],
+                              tcFloats[k], tcWhy[k]);
 
         if (hostOnly())
         {

@@ -207,6 +207,9 @@ struct TcLayer
     int  b;              // float offset of the bias (outP) in the element's
                          // float region
     int  fp;             // tensor-memory column of this layer's f' values
+    int  splitF, splitB; // operands of the forward (W) / backward (W^T) GEMM
+                         // of this layer: 0 single BF16, 1 weights hi/lo
+                         // (2 MMAs per K-step), 2 both hi/lo (3 MMAs)
 };
 
 struct TcNet
@@ -229,7 +232,8 @@ struct TcNNParams
     int   maxP;                   // widest padded width (A tile columns)
     int   wMax;                   // bytes reserved for weights in smem
     int   fMax;                   // floats reserved for the float region
-    int   split;                  // 1: hi/lo BF16 operands (3 MMAs / step)
+    int   split;                  // 1: some GEMM splits its activations
+                                  // (the low operand tile is allocated)
     int   tmemCols;               // tensor-memory columns allocated per CTA
                                   // (accumulators, then the f' columns)
     int   smemBytes;              // dynamic shared memory per CTA
@@ -259,7 +263,10 @@ struct TcNNLaunch
 void launchNeuralNetworksTC(TcNNParams const& P, TcNNLaunch const& L,
                             cudaStream_t s);
 // Builds the tensor-core tables and blobs from the FP64 weight blob; false
-// (with the reason) if a network does not fit the kernel.
+// (with the reason) if a network does not fit the kernel.  split: 0 = single
+// BF16 operands everywhere, 1 = hi/lo activations and weights in every
+// GEMM, 2 = the same except the backward GEMMs of the hidden layers above
+// the first, whose deltas stay single BF16 (their weights hi/lo).
 bool tcBuild(NNParams const& nn, std::vector<double> const& blob, int split,
              TcNNParams& P, std::vector<unsigned char>& wblob,
              std::vector<float>& fblob, std::string& why);

@@ -289,10 +289,11 @@ __device__ __forceinline__ void actF(int a, float x, float& v, float& dv)
     }
 }
 
-// One GEMM D[128 x nP] = A[128 x kP] B[nP x kP]^T into tensor memory, with
-// split operands D = Ah Bh + Ah Bl + Al Bh.  All threads call it after
-// writing their operand rows; returns false (for every thread) when the
-// completion wait gave up.
+// One GEMM D[128 x nP] = A[128 x kP] B[nP x kP]^T into tensor memory:
+// split 0: D = Ah Bh; 1 (weights split): D = Ah Bh + Ah Bl; 2 (both
+// split): D = Ah Bh + Ah Bl + Al Bh.  All threads call it after writing
+// their operand rows; returns false (for every thread) when the completion
+// wait gave up.
 __device__ __forceinline__ bool tcGemm(uint32_t tmemD, uint32_t aH,
                                        uint32_t aL, uint32_t bH, uint32_t bL,
                                        int kP, int nP, int split, uint32_t bar,
@@ -312,11 +313,10 @@ __device__ __forceinline__ bool tcGemm(uint32_t tmemD, uint32_t aH,
             uint64_t const ah = ummaDesc(aH + o, 128, sbo);
             uint64_t const bh = ummaDesc(bH + o, 128, sbo);
             mmaBF16(tmemD, ah, bh, id, s > 0 ? 1u : 0u);
-            if (split)
-            {
+            if (split >= 1)
                 mmaBF16(tmemD, ah, ummaDesc(bL + o, 128, sbo), id, 1u);
+            if (split >= 2)
                 mmaBF16(tmemD, ummaDesc(aL + o, 128, sbo), bh, id, 1u);
-            }
         }
         mmaCommit(bar);
     }
@@ -423,7 +423,7 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
                 __nv_bfloat16 const h = __float2bfloat16_rn(v);
                 int const off = aOff(row, k, N.ninP);
                 *reinterpret_cast<__nv_bfloat16*>(sAh + off) = h;
-                if (P.split)
+                if (N.layer[0].splitF == 2)
                     *reinterpret_cast<__nv_bfloat16*>(sAl + off) =
                         __float2bfloat16_rn(v - __bfloat162float(h));
             }
@@ -435,7 +435,7 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
         {
             TcLayer const& Ly = N.layer[l];
             ok = tcGemm(tmem, aH, aL, w0 + Ly.w, w0 + Ly.wl, Ly.inP, Ly.outP,
-                        P.split, bar, phase, sAbort);
+                        Ly.splitF, bar, phase, sAbort);
             if (!ok) break;
             float const* b = sF + Ly.b;
             bool const last = (l == N.hidden - 1);
@@ -452,7 +452,9 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
                     d[q] = da;
                 }
                 tmemSt16(tRow + Ly.fp + c0, d);
-                if (!last) store16(sAh, sAl, r, c0, Ly.outP, v);
+                if (!last)
+                    store16(sAh, N.layer[l + 1].splitF == 2 ? sAl : nullptr,
+                            r, c0, Ly.outP, v);
                 else
                 {
 #pragma unroll
@@ -478,14 +480,15 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
 #pragma unroll
                 for (int q = 0; q < 16; ++q)
                     v[q] *= dEz * sF[N.outW + c0 + q];
-                store16(sAh, sAl, r, c0, LH.outP, v);
+                store16(sAh, LH.splitB == 2 ? sAl : nullptr, r, c0, LH.outP,
+                        v);
             }
         }
         for (int l = N.hidden - 1; l >= 0 && ok; --l)
         {
             TcLayer const& Ly = N.layer[l];
             ok = tcGemm(tmem, aH, aL, w0 + Ly.wt, w0 + Ly.wtl, Ly.outP,
-                        Ly.inP, P.split, bar, phase, sAbort);
+                        Ly.inP, Ly.splitB, bar, phase, sAbort);
             if (!ok) break;
             if (l > 0)
             {
@@ -497,7 +500,8 @@ nnTcKernel(__grid_constant__ TcNNParams const P,
                     tmemLd16(tRow + Lp.fp + c0, d);
 #pragma unroll
                     for (int q = 0; q < 16; ++q) v[q] *= d[q];
-                    store16(sAh, sAl, r, c0, Ly.inP, v);
+                    store16(sAh, Lp.splitB == 2 ? sAl : nullptr, r, c0,
+                            Ly.inP, v);
                 }
             }
             else
@@ -589,7 +593,7 @@ bool tcBuild(NNParams const& nn, std::vector<double> const& blob, int split,
     wblob.clear();
     fblob.clear();
     P.numElements = nn.numElements;
-    P.split = split ? 1 : 0;
+    P.split = split ? 1 : 0;   // some activations split: the low tile
     auto pad16 = [](int x) { return (x + 15) / 16 * 16; };
     int maxP = 16, wMax = 0, fMax = 0, accCols = 16, fpCols = 0;
     for (int e = 0; e < nn.numElements; ++e)
@@ -641,14 +645,18 @@ bool tcBuild(NNParams const& nn, std::vector<double> const& blob, int split,
             int const ni = Ly.in;
             auto w = [&](int o, int j) { return W[(long)o * ni + j] * norm; };
             auto wt = [&](int j, int o) { return W[(long)o * ni + j] * norm; };
+            // Per GEMM: 2 = activations and weights split, 1 = weights only.
+            Ly.splitF = split ? 2 : 0;
+            Ly.splitB = (split == 1 || (split == 2 && h == 0)) ? 2
+                      : (split == 2) ? 1 : 0;
             Ly.w = append(ummaTile(Ly.out, Ly.in, Ly.outP, Ly.inP, false, w));
-            Ly.wl = split ? append(ummaTile(Ly.out, Ly.in, Ly.outP, Ly.inP,
-                                            true, w))
-                          : Ly.w;
+            Ly.wl = Ly.splitF ? append(ummaTile(Ly.out, Ly.in, Ly.outP,
+                                                Ly.inP, true, w))
+                              : Ly.w;
             Ly.wt = append(ummaTile(Ly.in, Ly.out, Ly.inP, Ly.outP, false, wt));
-            Ly.wtl = split ? append(ummaTile(Ly.in, Ly.out, Ly.inP, Ly.outP,
-                                             true, wt))
-                           : Ly.wt;
+            Ly.wtl = Ly.splitB ? append(ummaTile(Ly.in, Ly.out, Ly.inP,
+                                                 Ly.outP, true, wt))
+                               : Ly.wt;
             Ly.b = (int)freg.size();
             for (int o = 0; o < Ly.outP; ++o)
                 freg.push_back(o < Ly.out ? (float)(b[o] * norm) : 0.0f);

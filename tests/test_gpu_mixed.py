@@ -76,10 +76,14 @@ def test_mixed_intermediates(gpu, name, mode):
     assert _rel_rms(E1, E0) < tol
 
 
+@pytest.mark.parametrize("mode", ["mixed", "bf16"])
 @pytest.mark.parametrize("name,nmol,seed", [("h2o_52", 512, 5),
                                             ("h2o_92", 512, 6)])
-def test_mixed_energy_force_rmse(gpu, name, nmol, seed):
-    p, ref = _pair(name)
+def test_mixed_energy_force_rmse(gpu, name, nmol, seed, mode):
+    """Both tensor-core forms meet the targets: hi/lo operands everywhere
+    (mixed), or single BF16 deltas in the hidden layers' backward GEMMs
+    (bf16)."""
+    p, ref = _pair(name, mode)
     box, pos, elem = synth.water_box(nmol, seed)
     n = len(pos)
     rng = np.random.default_rng(seed)
@@ -93,7 +97,8 @@ def test_mixed_energy_force_rmse(gpu, name, nmol, seed):
         dF.append((f1 - f0).ravel())
     e_rmse = float(np.sqrt(np.mean(np.square(dE))))
     f_rmse = float(np.sqrt(np.mean(np.square(np.concatenate(dF)))))
-    print(f"{name}: energy/atom RMSE {e_rmse:.3e}, force RMSE {f_rmse:.3e}")
+    print(f"{name} {mode}: energy/atom RMSE {e_rmse:.3e}, "
+          f"force RMSE {f_rmse:.3e}")
     assert e_rmse <= E_PER_ATOM_RMSE
     assert f_rmse <= F_RMSE
 
