@@ -131,6 +131,13 @@ public:
         log << std::string(line);
     }
 
+    // InterfaceLammps::writeExtrapolationWarnings (InterfaceLammps.cpp:
+    // 751-765): the recorded warnings' lines through the log.
+    void writeExtrapolationWarnings() override
+    {
+        log << getExtrapolationWarningLines();
+    }
+
     Log log;
 
 private:

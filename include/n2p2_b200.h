@@ -264,6 +264,26 @@ int64_t n2p2b_get_num_extrapolation_warnings(const n2p2b_context* ctx);
 int     n2p2b_reset_extrapolation_warnings(n2p2b_context* ctx);
 /* Warnings per atom of the last evaluation (num_atoms ints). */
 int     n2p2b_get_extrapolation_counts(n2p2b_context* ctx, int32_t* counts);
+/* The warnings of the last evaluation, one record each, in the order the
+ * reference records them (atom by atom, each atom's symmetry functions in
+ * order; Element::updateSymmetryFunctionStatistics, libnnp/Element.cpp:
+ * 462-541, with the fields of SymFncStatistics::addExtrapolationWarning,
+ * libnnp/SymFncStatistics.cpp:91-110).  At most `capacity` records into
+ * `out`; *count receives their number (also when it is larger). */
+typedef struct n2p2b_extrapolation_warning
+{
+    int64_t atom;      /* atom index in the structure (0-based) */
+    int32_t element;   /* element index */
+    int32_t sf;        /* symmetry function, element-local index (0-based) */
+    int32_t type;      /* symmetry-function type */
+    int32_t reserved;
+    double  value;     /* unscaled value */
+    double  gmin;      /* scaling.data minimum */
+    double  gmax;      /* scaling.data maximum */
+} n2p2b_extrapolation_warning;
+int n2p2b_get_extrapolation_warnings(n2p2b_context* ctx, int64_t capacity,
+                                     n2p2b_extrapolation_warning* out,
+                                     int64_t* count);
 
 /* ---- distilled student network --------------------------------------- */
 

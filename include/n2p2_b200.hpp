@@ -23,6 +23,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdint>
+#include <cstring>
 #include <fstream>
 #include <map>
 #include <sstream>
@@ -437,9 +438,12 @@ public:
         loadSettingsFile(dir + "input.nn");
         setupGeneric();
         setupSymmetryFunctionScaling(dir + "scaling.data");
+        // As the reference: warnings are collected (not written while the
+        // symmetry functions are computed); writeExtrapolationWarnings
+        // writes them.
         setupSymmetryFunctionStatistics(false, showew || showewsum > 0
                                                    || maxew >= 0,
-                                        showew, false);
+                                        false, false);
         setupNeuralNetworkWeights(dir + "weights.%03zu.data");
         if (lammpsCutoff < getMaxCutoffRadiusLammps())
             throw std::runtime_error("ERROR: LAMMPS cutoff via pair_coeff "
@@ -512,8 +516,16 @@ public:
         maxTarget_ = numAtomsLocal;
         finalized_ = false;
     }
-    void setLocalTags(int const* const) {}
-    void setLocalTags(int64_t const* const) {}
+    // InterfaceLammps::setLocalTags (InterfaceLammps.cpp:325-345): the
+    // LAMMPS tags of the local atoms, the atom field of the warnings.
+    void setLocalTags(int const* const atomTag)
+    {
+        tags_.assign(atomTag, atomTag + nlocal_);
+    }
+    void setLocalTags(int64_t const* const atomTag)
+    {
+        tags_.assign(atomTag, atomTag + nlocal_);
+    }
     void allocateNeighborlists(int const* const numneigh)
     {
         for (int i = 0; i < nlocal_; ++i)
@@ -573,9 +585,7 @@ public:
         check(ctx_, n2p2b_get_atomic_energies(ctx_, atomEnergy_.data()));
         forces_.resize(3 * (std::size_t)maxTarget_);
         check(ctx_, n2p2b_get_target_forces(ctx_, forces_.data()));
-        if (maxew_ > 0 && getNumExtrapolationWarnings() > (std::size_t)maxew_)
-            throw std::out_of_range("ERROR: Too many extrapolation "
-                                    "warnings.\n");
+        if (showew_) collectExtrapolationWarnings();
     }
     double getEnergy() const { return energy_ / cfenergy_; }
     double getAtomicEnergy(int index) const
@@ -594,27 +604,136 @@ public:
             for (int c = 0; c < 3; ++c)
                 atomF[m][c] += forces_[3 * (std::size_t)m + c] * cf;
     }
-    // Extrapolation-warning output (InterfaceLammps.cpp:638-776).  With
-    // showew the library writes the reference's warning lines
-    // (Element.cpp:505-518) while process() runs, so
-    // writeExtrapolationWarnings has nothing left to write.  The reference's
-    // EW buffers carry per-SF statistics records from the other MPI ranks
-    // to rank 0; here every rank writes its own lines, so no records travel
-    // and the buffer is empty (as in the reference built without MPI).
-    long getEWBufferSize() const { return 0; }
+    // Extrapolation-warning output (InterfaceLammps.cpp:638-776).  process()
+    // records this rank's warnings per element and symmetry function (the
+    // SymFncStatistics containers, SymFncStatistics.cpp:91-137: type, range,
+    // and per warning the structure index, the atom's LAMMPS tag and the
+    // value); the pair style moves other ranks' records to rank 0 through
+    // the EW buffer (getEWBufferSize / fillEWBuffer / extractEWBuffer, a
+    // plain byte layout of the same fields) and has rank 0 write them.
+    long getEWBufferSize() const
+    {
+        long bs = 0;
+        for (auto const& m : ewData_)
+        {
+            bs += 8;
+            for (auto const& kv : m)
+            {
+                EWContainer const& d = kv.second;
+                bs += 8 * 3 + 8 * 2 + 8 + (long)d.element.size() + 1;
+                bs += (long)d.valueEW.size() * (8 + 8 + 8);
+            }
+        }
+        return bs;
+    }
     void fillEWBuffer(char* const& buf, int bs) const
     {
-        (void)buf;
-        (void)bs;
+        std::size_t p = 0;
+        auto put = [&](void const* v, std::size_t k) {
+            if (p + k > (std::size_t)bs)
+                throw std::out_of_range("ERROR: EW buffer too small.\n");
+            std::memcpy(buf + p, v, k);
+            p += k;
+        };
+        for (auto const& m : ewData_)
+        {
+            uint64_t const n = m.size();
+            put(&n, 8);
+            for (auto const& kv : m)
+            {
+                EWContainer const& d = kv.second;
+                uint64_t const h[3] = {kv.first, d.valueEW.size(), d.type};
+                put(h, sizeof(h));
+                put(&d.gmin, 8);
+                put(&d.gmax, 8);
+                uint64_t const ts = d.element.size() + 1;
+                put(&ts, 8);
+                put(d.element.c_str(), ts);
+                put(d.structureEW.data(), 8 * d.valueEW.size());
+                put(d.atomEW.data(), 8 * d.valueEW.size());
+                put(d.valueEW.data(), 8 * d.valueEW.size());
+            }
+        }
     }
     void extractEWBuffer(char const* const& buf, int bs)
     {
-        (void)buf;
-        (void)bs;
+        std::size_t p = 0;
+        auto get = [&](void* v, std::size_t k) {
+            if (p + k > (std::size_t)bs)
+                throw std::out_of_range("ERROR: EW buffer truncated.\n");
+            std::memcpy(v, buf + p, k);
+            p += k;
+        };
+        ewData_.resize(numElements());
+        for (auto& m : ewData_)
+        {
+            uint64_t n = 0;
+            get(&n, 8);
+            for (uint64_t i = 0; i < n; ++i)
+            {
+                uint64_t h[3];
+                get(h, sizeof(h));
+                EWContainer& d = m[(std::size_t)h[0]];
+                d.type = (std::size_t)h[2];
+                get(&d.gmin, 8);
+                get(&d.gmax, 8);
+                uint64_t ts = 0;
+                get(&ts, 8);
+                std::string el(ts, '\0');
+                get(&el[0], ts);
+                d.element = el.c_str();
+                std::size_t const c = d.valueEW.size(), k = (std::size_t)h[1];
+                d.structureEW.resize(c + k);
+                d.atomEW.resize(c + k);
+                d.valueEW.resize(c + k);
+                get(d.structureEW.data() + c, 8 * k);
+                get(d.atomEW.data() + c, 8 * k);
+                get(d.valueEW.data() + c, 8 * k);
+            }
+        }
     }
-    void writeExtrapolationWarnings() {}
-    // SymFncStatistics::clear on every element: the warnings and their count.
-    void clearExtrapolationWarnings() { resetExtrapolationWarnings(); }
+    // SymFncStatistics::getExtrapolationWarningLines for every element
+    // (SymFncStatistics.cpp:112-137): element by element, symmetry function
+    // by symmetry function, warnings in the order they were recorded.
+    std::vector<std::string> getExtrapolationWarningLines() const
+    {
+        std::vector<std::string> vs;
+        for (auto const& m : ewData_)
+            for (auto const& kv : m)
+            {
+                EWContainer const& d = kv.second;
+                for (std::size_t i = 0; i < d.valueEW.size(); ++i)
+                {
+                    char line[256];
+                    std::snprintf(line, sizeof(line),
+                                  "### NNP EXTRAPOLATION WARNING ### "
+                                  "STRUCTURE: %6zu ATOM: %9zu ELEMENT: %2s "
+                                  "SYMFUNC: %4zu TYPE: %2zu VALUE: %10.3E "
+                                  "MIN: %10.3E MAX: %10.3E\n",
+                                  (std::size_t)d.structureEW[i],
+                                  (std::size_t)d.atomEW[i],
+                                  d.element.c_str(), kv.first + 1, d.type,
+                                  d.valueEW[i], d.gmin, d.gmax);
+                    vs.push_back(line);
+                }
+            }
+        return vs;
+    }
+    // InterfaceLammps::writeExtrapolationWarnings writes to the interface's
+    // log; this class has none and writes to stderr (nnp::InterfaceLammps
+    // in InterfaceLammps.h writes to its log).
+    virtual void writeExtrapolationWarnings()
+    {
+        for (std::string const& l : getExtrapolationWarningLines())
+            std::fputs(l.c_str(), stderr);
+    }
+    // SymFncStatistics::clear on every element: the records and the count.
+    void clearExtrapolationWarnings()
+    {
+        ewData_.clear();
+        resetExtrapolationWarnings();
+    }
+    virtual ~InterfaceLammps() = default;
 
     // InterfaceLammps::getMaxCutoffRadius (InterfaceLammps.cpp:489-493):
     // the largest symmetry-function cutoff in LAMMPS units (the pair style
@@ -628,16 +747,56 @@ public:
     }
 
 private:
+    // The warnings of the last evaluation into the per-element records;
+    // the atom field is the atom's LAMMPS tag (its local index + 1 when no
+    // tags were set), the structure index 0.
+    void collectExtrapolationWarnings()
+    {
+        int64_t cnt = 0;
+        check(ctx_, n2p2b_get_extrapolation_warnings(ctx_, 0, nullptr, &cnt));
+        if (cnt == 0) return;
+        std::vector<n2p2b_extrapolation_warning> w((std::size_t)cnt);
+        check(ctx_, n2p2b_get_extrapolation_warnings(ctx_, cnt, w.data(),
+                                                     &cnt));
+        ewData_.resize(numElements());
+        for (n2p2b_extrapolation_warning const& x : w)
+        {
+            int const li = lammpsIndex_.at((std::size_t)x.atom);
+            int64_t const tag = li < (int)tags_.size() ? tags_[li] : li + 1;
+            EWContainer& d = ewData_[x.element][(std::size_t)x.sf];
+            d.type = (std::size_t)x.type;
+            d.gmin = x.gmin;
+            d.gmax = x.gmax;
+            d.element = elementSymbol(x.element);
+            d.structureEW.push_back(0);
+            d.atomEW.push_back((uint64_t)tag);
+            d.valueEW.push_back(x.value);
+        }
+    }
+
+    struct EWContainer
+    {
+        std::size_t           type = 0;
+        double                gmin = 0.0, gmax = 0.0;
+        std::string           element;
+        std::vector<uint64_t> structureEW, atomEW;
+        std::vector<double>   valueEW;
+    };
     struct Entry
     {
         int    j;
         int    element;
         double dx, dy, dz;
     };
+    std::vector<int64_t>                          tags_;
+    std::vector<std::map<std::size_t, EWContainer>> ewData_;
     bool                            initialized_ = false;
     bool                            finalized_ = false;
     bool                            showew_ = false, resetew_ = false;
-    int                             maxew_ = 0;
+    int                             maxew_ = 0;  // enforced by the pair
+                                                 // style (pair_hdnnp.cpp:
+                                                 // 358-361), as for the
+                                                 // reference
     double                          cflength_ = 1.0, cfenergy_ = 1.0;
     int                             myRank_ = 0;
     std::map<int, int>              typeToElement_;

@@ -48,6 +48,8 @@ SIGNATURES = {
     "n2p2b_get_num_extrapolation_warnings": (C.c_int64, [_vp]),
     "n2p2b_reset_extrapolation_warnings": (C.c_int, [_vp]),
     "n2p2b_get_extrapolation_counts": (C.c_int, [_vp, _i32p]),
+    "n2p2b_get_extrapolation_warnings": (C.c_int, [_vp, C.c_int64, _vp,
+                                                   _i64p]),
     "n2p2b_set_structures": (C.c_int, [_vp, C.c_int64, _i64p, _vp, _vp,
                                        C.c_int, _i32p, C.c_int]),
     "n2p2b_get_structure_energies": (C.c_int, [_vp, _dp]),

@@ -1289,15 +1289,18 @@ struct n2p2b_context
                                      "out of range.\n");
     }
 
-    // The reference's warning lines (Element.cpp:505-518) for the last
-    // evaluation; prints all of them when `print`, returns the first.
-    std::string ewLines(bool print)
+    // The warnings of the last evaluation as the reference records them
+    // (Element::updateSymmetryFunctionStatistics, Element.cpp:462-541, atom
+    // by atom, each atom's symmetry functions in order): the unscaled value
+    // (SymFnc::unscale of the kernel's G) outside [Gmin, Gmax] by more than
+    // 1000 DBL_EPSILON.
+    std::vector<n2p2b_extrapolation_warning> ewRecords()
     {
+        std::vector<n2p2b_extrapolation_warning> out;
         std::vector<int> per(n);
         ck(cudaMemcpy(per.data(), ewPerAtom.p, sizeof(int) * n,
                       cudaMemcpyDeviceToHost), "read warnings");
         std::vector<double> const g = readReal(G, (std::size_t)n * maxSF);
-        std::string first;
         double const eps = 1000.0 * DBL_EPSILON;
         for (long i = 0; i < n; ++i)
         {
@@ -1311,17 +1314,38 @@ struct n2p2b_context
                 double const v = (g[(std::size_t)i * maxSF + s] - q.smin) / q.b
                                + q.shift;
                 if (!(v + eps < r.lo || v - eps > r.hi)) continue;
-                char buf[256];
-                std::snprintf(buf, sizeof(buf),
-                              "### NNP EXTRAPOLATION WARNING ### STRUCTURE: "
-                              "%6zu ATOM: %9ld ELEMENT: %2s SYMFUNC: %4zu "
-                              "TYPE: %2d VALUE: %10.3E MIN: %10.3E MAX: "
-                              "%10.3E\n", (std::size_t)0, i,
-                              el.symbol.c_str(), s + 1, el.sfs[s].type, v,
-                              r.lo, r.hi);
-                if (first.empty()) first = buf;
-                if (print) std::fputs(buf, stderr);
+                n2p2b_extrapolation_warning w{};
+                w.atom = i;
+                w.element = e;
+                w.sf = (int32_t)s;
+                w.type = el.sfs[s].type;
+                w.value = v;
+                w.gmin = r.lo;
+                w.gmax = r.hi;
+                out.push_back(w);
             }
+        }
+        return out;
+    }
+
+    // The reference's warning lines (Element.cpp:505-518) for the last
+    // evaluation; prints all of them when `print`, returns the first.
+    std::string ewLines(bool print)
+    {
+        std::string first;
+        for (n2p2b_extrapolation_warning const& w : ewRecords())
+        {
+            Element const& el = pot.elements[w.element];
+            char buf[256];
+            std::snprintf(buf, sizeof(buf),
+                          "### NNP EXTRAPOLATION WARNING ### STRUCTURE: "
+                          "%6zu ATOM: %9ld ELEMENT: %2s SYMFUNC: %4zu "
+                          "TYPE: %2d VALUE: %10.3E MIN: %10.3E MAX: "
+                          "%10.3E\n", (std::size_t)0, (long)w.atom,
+                          el.symbol.c_str(), (std::size_t)w.sf + 1, w.type,
+                          w.value, w.gmin, w.gmax);
+            if (first.empty()) first = buf;
+            if (print) std::fputs(buf, stderr);
         }
         return first;
     }
@@ -2686,6 +2710,26 @@ int n2p2b_get_extrapolation_counts(n2p2b_context* ctx, int32_t* counts)
         ctx->activate();
         ck(cudaMemcpy(counts, ctx->ewPerAtom.p, sizeof(int32_t) * ctx->n,
                       cudaMemcpyDeviceToHost), "read warnings");
+    });
+}
+
+int n2p2b_get_extrapolation_warnings(n2p2b_context* ctx, int64_t capacity,
+                                     n2p2b_extrapolation_warning* out,
+                                     int64_t* count)
+{
+    return guarded(ctx, [&] {
+        if (!ctx->haveEW || !ctx->ewCheck)
+            throw StateError("ERROR: No extrapolation check ran (enable it "
+                             "with n2p2b_setup_symmetry_function_statistics)."
+                             "\n");
+        if (count == nullptr || capacity < 0 || (capacity > 0 && !out))
+            throw std::invalid_argument("ERROR: warning buffer");
+        ctx->activate();
+        std::vector<n2p2b_extrapolation_warning> const w = ctx->ewRecords();
+        *count = (int64_t)w.size();
+        std::size_t const k = std::min<std::size_t>(w.size(),
+                                                    (std::size_t)capacity);
+        if (k) std::memcpy(out, w.data(), k * sizeof(w[0]));
     });
 }
 

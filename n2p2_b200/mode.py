@@ -305,6 +305,25 @@ class Mode:
             self._h, out.ctypes.data_as(C.POINTER(C.c_int32))))
         return out
 
+    # Record layout of n2p2b_extrapolation_warning (include/n2p2_b200.h).
+    EW_DTYPE = np.dtype([("atom", np.int64), ("element", np.int32),
+                         ("sf", np.int32), ("type", np.int32),
+                         ("reserved", np.int32), ("value", np.float64),
+                         ("gmin", np.float64), ("gmax", np.float64)])
+
+    def extrapolation_warnings(self):
+        """The warnings of the last evaluation as records (atom, element,
+        sf (0-based), type, value, gmin, gmax), in the reference's order."""
+        cnt = C.c_int64(0)
+        self._check(self._L.n2p2b_get_extrapolation_warnings(
+            self._h, 0, None, C.byref(cnt)))
+        out = np.zeros(cnt.value, dtype=self.EW_DTYPE)
+        if cnt.value:
+            self._check(self._L.n2p2b_get_extrapolation_warnings(
+                self._h, cnt.value, out.ctypes.data_as(C.c_void_p),
+                C.byref(cnt)))
+        return out
+
     # ---- distilled student ------------------------------------------------
     _STUDENT_MODES = {"off": _capi.STUDENT_OFF, "gated": _capi.STUDENT_GATED,
                       "only": _capi.STUDENT_ONLY}

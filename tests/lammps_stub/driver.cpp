@@ -4,7 +4,7 @@
 // and the single-rank LAMMPS stand-in headers of include/ here -- on one
 // periodic structure, the way LAMMPS runs a pair style for one step:
 //
-//   pair_style hdnnp <cutoff> dir <potential> showew no maxew 1000000000
+//   pair_style hdnnp <cutoff> dir <potential> showew no|yes maxew 1000000000
 //                    [cflength <a> cfenergy <b>]
 //   pair_coeff * * <element symbols in input.nn order>
 //   init_style (neighbor request, interface setup), compute(eflag, vflag)
@@ -16,12 +16,17 @@
 // reverse communication).  Positions are in LAMMPS units: the potential's
 // length unit divided by cflength.
 //
-//   lammps_pair_hdnnp <potential dir> <input.data> [cflength cfenergy]
+//   lammps_pair_hdnnp <potential dir> <input.data> [cflength cfenergy [showew]]
 //
 // Prints "energy E", "virial v0..v5", and "force i fx fy fz" / "eatom i e"
 // per atom (LAMMPS units), plus "requests n flags f" of the neighbor
 // request and "log <line>" for each line the interface wrote to the
-// registered screen file.
+// registered screen file.  With "showew" the pair style shows individual
+// extrapolation warnings (atom tags = index + 1); the interface then runs
+// process() once more and moves its warning records through the EW buffer
+// (getEWBufferSize, fillEWBuffer, clearExtrapolationWarnings,
+// extractEWBuffer), printing the lines it holds afterwards as
+// "ewbuf <line>".
 #include "pair_hdnnp.h"
 
 #include "atom.h"
@@ -31,6 +36,7 @@
 #include "memory.h"
 #include "neighbor.h"
 #include "update.h"
+#include "InterfaceLammps.h"
 #include "n2p2_b200.hpp"
 
 #include <cmath>
@@ -48,14 +54,15 @@ using namespace LAMMPS_NS;
 
 int main(int argc, char* argv[])
 {
-    if (argc != 3 && argc != 5)
+    if (argc != 3 && argc != 5 && argc != 6)
     {
         std::fprintf(stderr, "USAGE: %s <potential dir> <input.data> "
-                             "[cflength cfenergy]\n", argv[0]);
+                             "[cflength cfenergy [showew]]\n", argv[0]);
         return 1;
     }
-    std::string const cfl = argc == 5 ? argv[3] : "1.0";
-    std::string const cfe = argc == 5 ? argv[4] : "1.0";
+    std::string const cfl = argc >= 5 ? argv[3] : "1.0";
+    std::string const cfe = argc >= 5 ? argv[4] : "1.0";
+    bool const showew = argc == 6 && std::string(argv[5]) == "showew";
     double const cflength = std::atof(cfl.c_str());
     try
     {
@@ -206,9 +213,16 @@ int main(int argc, char* argv[])
         list.numneigh = numneigh.data();
         list.firstneigh = firstneigh.data();
 
-        PairHDNNP pair(&lmp);
+        // The pair style's interface member, for the EW buffer round trip.
+        struct PairAccess : PairHDNNP
+        {
+            using PairHDNNP::PairHDNNP;
+            nnp::InterfaceLammps* iface() { return interface; }
+        };
+        PairAccess pair(&lmp);
         std::string const rcs = std::to_string(rcut);
-        std::vector<std::string> sa = {rcs, "dir", argv[1], "showew", "no",
+        std::vector<std::string> sa = {rcs, "dir", argv[1], "showew",
+                                       showew ? "yes" : "no",
                                        "maxew", "1000000000", "cflength",
                                        cfl, "cfenergy", cfe};
         std::vector<char*> sv;
@@ -242,6 +256,21 @@ int main(int argc, char* argv[])
         while (std::fgets(line, sizeof(line), lmp.screen))
             std::printf("log %s", line);
         std::fclose(lmp.screen);
+        if (showew)
+        {
+            nnp::InterfaceLammps* const in = pair.iface();
+            in->process();
+            long const bs = in->getEWBufferSize();
+            std::vector<char> buf((std::size_t)bs + 1);
+            char* const bp = buf.data();
+            in->fillEWBuffer(bp, (int)bs);
+            in->clearExtrapolationWarnings();
+            char const* const cbp = buf.data();
+            in->extractEWBuffer(cbp, (int)bs);
+            for (std::string const& l : in->getExtrapolationWarningLines())
+                std::printf("ewbuf %s", l.c_str());
+            std::printf("ewbytes %ld\n", bs);
+        }
     }
     catch (std::exception const& e)
     {

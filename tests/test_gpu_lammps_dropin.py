@@ -79,3 +79,63 @@ def test_pair_hdnnp_unchanged_matches_reference(gpu, tmp_path, cf):
     fs = np.maximum(np.abs(f0), np.sqrt(np.mean(f0 ** 2)))
     assert np.all(np.abs(f * cfe / cfl - f0) <= 1e-10 * fs)
     assert np.abs(ea * cfe - a0).max() <= 1e-10 * np.abs(a0).max()
+
+
+def _warning_fields(line):
+    """(structure, atom, element, symfunc, type, value, min, max) of a
+    "### NNP EXTRAPOLATION WARNING ###" line."""
+    t = line.split()
+    k = {t[i].rstrip(":"): t[i + 1] for i in range(5, len(t) - 1, 2)}
+    return (int(k["STRUCTURE"]), int(k["ATOM"]), k["ELEMENT"],
+            int(k["SYMFUNC"]), int(k["TYPE"]), float(k["VALUE"]),
+            k["MIN"], k["MAX"])
+
+
+def test_pair_hdnnp_extrapolation_warnings(gpu, tmp_path):
+    """showew: the pair style writes the interface's warning lines through
+    the log (InterfaceLammps::writeExtrapolationWarnings), element by
+    element, symmetry function by symmetry function, with the LAMMPS tags
+    as atom field -- the lines the reference writes for the same
+    configuration, its G tested against scaling.data's range.  The EW
+    buffer (fill, clear, extract) carries the same records."""
+    from oracle.ref import RefModel
+    box, pos, elem = synth.water_box(32, 23)
+    box, pos = box * 0.92, np.mod(pos * 0.92, box[0, 0] * 0.92)
+    _write(tmp_path / "input.data", box, pos, elem)
+    r = subprocess.run([EXE, POT, str(tmp_path / "input.data"), "1.0", "1.0",
+                        "showew"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    lines = r.stdout.split("\n")
+    got = [ln[4:] for ln in lines
+           if ln.startswith("log ### NNP EXTRAPOLATION WARNING ###")]
+    buf = [ln[6:] for ln in lines
+           if ln.startswith("ewbuf ### NNP EXTRAPOLATION WARNING ###")]
+    assert got and buf == got
+
+    ref = RefModel(POT)
+    ref.setup_statistics(collect_ew=True)
+    ref.set_structure(pos, elem, box)
+    ref.evaluate(True)
+    assert len(got) == ref.num_extrapolation_warnings()
+    # The reference's records: per element, per symmetry function, per atom.
+    rows = [ln.split() for ln in open(os.path.join(POT, "scaling.data"))
+            if ln.strip() and not ln.lstrip().startswith("#")]
+    sc = {(int(q[0]) - 1, int(q[1]) - 1): [float(x) for x in q[2:5]]
+          for q in rows}
+    G = ref.G()
+    eps = 1000.0 * np.finfo(float).eps
+    want = []
+    for e in range(2):
+        for s in range(ref.num_sf[e]):
+            gmin, gmax, gmean = sc[(e, s)]
+            for i in np.flatnonzero(elem == e):
+                v = G[i, s] + gmean        # center-only scaling
+                if v + eps < gmin or v - eps > gmax:
+                    want.append((0, int(i) + 1, SYM[e], s + 1,
+                                 int(ref.sf_params(e, s)[0]), v,
+                                 ("%10.3E" % gmin).strip(),
+                                 ("%10.3E" % gmax).strip()))
+    have = [_warning_fields(ln) for ln in got]
+    assert [w[:5] + w[6:] for w in have] == [w[:5] + w[6:] for w in want]
+    for h, w in zip(have, want):
+        assert abs(h[5] - w[5]) <= 5e-4 * abs(w[5])
