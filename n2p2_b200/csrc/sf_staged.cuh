@@ -49,8 +49,17 @@ constexpr int kStagedThreads = kThreads;   // 4 warps, one atom
 constexpr int kStagedWarps = kWarps;
 // eta runs per group the records hold (groups have at most this many).
 constexpr int kStagedRuns = 4;
-// Shared memory per CTA the record capacity is sized for: four CTAs per SM.
+// Shared memory per CTA the record capacity is sized for: four CTAs per SM
+// (N2P2B_SF_STAGED_KB overrides it, in KB, for measurements).
 constexpr long kStagedTargetBytes = 56L * 1024;
+inline long stagedTargetBytes()
+{
+    static long const v = [] {
+        char const* e = std::getenv("N2P2B_SF_STAGED_KB");
+        return e ? std::atol(e) * 1024L : kStagedTargetBytes;
+    }();
+    return v;
+}
 
 __host__ __device__ inline long align16(long b) { return (b + 15) / 16 * 16; }
 
@@ -128,25 +137,26 @@ inline bool stagedEligible(SFParams const& P, int ns)
 }
 
 // Record capacity: the largest multiple of 16 in [32, 96] whose CTA fits
-// kStagedTargetBytes (32 when none does).
+// stagedTargetBytes() (32 when none does).
 template <typename R>
 inline int stagedRecordCap(SFParams const& P, int cap, int ns, bool tables)
 {
     for (int rb = 96; rb > 32; rb -= 16)
-        if (stagedSharedBytes<R>(P, cap, ns, rb, tables) <= kStagedTargetBytes)
+        if (stagedSharedBytes<R>(P, cap, ns, rb, tables)
+            <= stagedTargetBytes())
             return rb;
     return 32;
 }
 
 // The tables are staged in shared memory when the CTA fits
-// kStagedTargetBytes with the smallest record capacity; larger tables (the
+// stagedTargetBytes() with the smallest record capacity; larger tables (the
 // 92-SF potential's) are read from global memory, which keeps four CTAs
 // per SM.
 template <typename R>
 inline bool stagedTablesShared(SFParams const& P, int cap, int ns)
 {
     return P.stageTables
-        && stagedSharedBytes<R>(P, cap, ns, 32, true) <= kStagedTargetBytes;
+        && stagedSharedBytes<R>(P, cap, ns, 32, true) <= stagedTargetBytes();
 }
 
 // Phase 1: the record of ordered triplet (owner t, partner k) of a group
