@@ -136,6 +136,8 @@ struct SFLaunch
                                       // warp batch (set by launcher)
     int            tablesShared = 0;  // staged kernel: group / member
                                       // tables staged in shared memory
+    int            lockstep = 1;      // staged kernel: the lockstep path
+                                      // for groups of at most 3 eta runs
     int const*     elem = nullptr;
     int const*     nbrOff = nullptr;
     int const*     nbrCountElem = nullptr;

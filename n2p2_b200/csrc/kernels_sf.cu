@@ -3,6 +3,7 @@
 // the context's precision (kernels_sf_{cos,tanhu,poly2,any}{,_f32}.cu,
 // templates in sf_impl.cuh).
 #include <algorithm>
+#include <cstdlib>
 
 #include "kernels.h"
 #include "sf_impl.cuh"
@@ -61,7 +62,7 @@ StagedGeom stagedGeomT(SFParams const& P, int cap, int ns)
     StagedGeom g;
     g.tables = sfk::stagedTablesShared<R>(P, cap, ns);
     g.rb = sfk::stagedRecordCap<R>(P, cap, ns, g.tables);
-    g.warpBytes = sfk::stagedWarpBytes<R>(P.maxSF, ns, g.rb);
+    g.warpBytes = sfk::stagedWarpBytes<R>(P.maxSF, ns, g.rb, cap);
     g.shm = sfk::stagedSharedBytes<R>(P, cap, ns, g.rb, g.tables);
     return g;
 }
@@ -148,6 +149,13 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,
                                         stagedShapes(L.variant));
         L.recCap = g.rb;
         L.tablesShared = g.tables ? 1 : 0;
+        // N2P2B_SF_LOCKSTEP=0 keeps the batched (member, slice) path for
+        // every narrow segment (measurements).
+        static int const lock = [] {
+            char const* e = std::getenv("N2P2B_SF_LOCKSTEP");
+            return e ? std::atoi(e) : 1;
+        }();
+        L.lockstep = lock;
         L.warpBytes = g.warpBytes;
         shm = g.shm;
     }

@@ -85,9 +85,12 @@ struct StagedCat
 };
 
 // Per-warp region: G sums, categories, batch list and tables, category
-// constants, records.
+// constants, records, and the lockstep path's partner lists (one list of
+// up to cap partners per owner of a group of 32 / ns owners), owner order
+// (cap entries) and its 32 sort buckets.
 template <typename R>
-__host__ __device__ inline long stagedWarpBytes(int maxSF, int ns, int rb)
+__host__ __device__ inline long stagedWarpBytes(int maxSF, int ns, int rb,
+                                                int cap)
 {
     long b = align16((long)sizeof(R) * maxSF);
     b += kCatsBytes;
@@ -95,6 +98,8 @@ __host__ __device__ inline long stagedWarpBytes(int maxSF, int ns, int rb)
     b += align16(ns == 4 ? (long)sizeof(StagedCat<R, 4>)
                          : (long)sizeof(StagedCat<R, 8>));
     b += align16((long)sizeof(R) * stagedStride(ns) * rb);
+    b += align16(2L * (32 / ns) * cap + 2L * cap);
+    b += 4L * 32;
     return b;
 }
 
@@ -115,7 +120,7 @@ __host__ __device__ inline long stagedSharedBytes(SFParams const& P, int cap,
 {
     return (tables ? (long)stagedTableBytes(P) : 0L)
          + stagedAtomBytes<R>(P.maxExp, cap)
-         + kStagedWarps * stagedWarpBytes<R>(P.maxSF, ns, rb);
+         + kStagedWarps * stagedWarpBytes<R>(P.maxSF, ns, rb, cap);
 }
 
 // The staged kernel serves potentials whose groups are radial or
@@ -396,6 +401,175 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
     }
 }
 
+// Eta runs per group the lockstep path keeps in registers.
+constexpr int kLockRuns = 3;
+
+// A product-form narrow angular segment [g0, g1) in lockstep: the warp runs
+// groups of J = 32 / NS owners of a category at once, and lane
+// (owner o = lane / NS, x = lane % NS) plays two roles per step of NS
+// partners:
+//   phase 1: the record of owner o's (step NS + x)-th valid partner;
+//   phase 2: the members (run a, shape x), a < runs, of owner o, summed
+//            over owner o's NS records of the step.
+// Every (owner, member) pair lives in one lane for the whole group: no
+// slice sums, one slot write per member when the group ends.  The group's
+// G values are added over its owners by a fixed butterfly.  Groups of a
+// category go to the warps round robin; an owner's partners come from a
+// list built from its validity mask (lanes of the owner split each mask
+// word).  Records of partners beyond an owner's count carry v = 0.  The
+// owners of a category are taken in the order of their partner counts
+// (descending; buildOwnerOrder), so that a group's owners need about the
+// same number of steps.
+template <typename R, int CT, int NS>
+__device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
+                                 DevMember const* M, int g0, int g1,
+                                 int const eb[kMaxElem + 1], int cnt,
+                                 int words, int capE, WarpMem<R> const& W,
+                                 StagedCat<R, NS>* cp, R* recs,
+                                 unsigned short* plist,
+                                 unsigned short* order, int* hist, int warp,
+                                 int warps, R* __restrict__ out,
+                                 int derivatives)
+{
+    constexpr int NF = stagedStride(NS);
+    constexpr int J = 32 / NS;
+    int const lane = threadIdx.x & 31;
+    int const o = lane / NS;
+    int const x = lane - o * NS;
+    unsigned short* const myList = plist + o * capE;
+    R* const myRec = recs + lane * NF;
+    int ncat = 0;
+    buildCats(G, g0, g1, eb, false, 0, W, ncat);
+    for (int c = 0; c < ncat; ++c)
+    {
+        Cat const cc = W.cats[c];
+        DevGroup const& g = G[cc.gi];
+        R const rc = R(g.rc);
+        int const nr = g.mcnt / NS;
+        bool const series = g.cosSeries != 0;
+        bool const pow16 = g.powBits <= 4;
+        if (lane == 0)
+        {
+            for (int s = 0; s < NS; ++s)
+            {
+                DevMember const& mm = M[g.mbeg + s];
+                cp->lam[s] = R(mm.lambda);
+                cp->zl[s] = R(mm.zetaLambda);
+                cp->zi[s] = mm.zetaInt;
+            }
+            for (int a = 0; a < kStagedRuns; ++a)
+            {
+                DevMember const& mm = M[g.mbeg + min(a, nr - 1) * NS];
+                cp->eta[a] = R(mm.eta);
+                cp->eoff[a] = mm.expIdx * capE;
+            }
+        }
+        __syncwarp();
+        StagedCat<R, NS> const& C = *cp;
+        R eta2[kLockRuns], eta4[kLockRuns];
+#pragma unroll
+        for (int a = 0; a < kLockRuns; ++a)
+        {
+            eta2[a] = R(2) * C.eta[a];
+            eta4[a] = R(4) * C.eta[a];
+        }
+        int const wb = cc.pb >> 5;
+        int const we = (cc.pe + 31) >> 5;
+        buildOwnerOrder(W, words, cc.ob, cc.ob + cc.on, cc.pb, cc.pe, order,
+                        hist);
+        __syncwarp();
+
+        for (int q0 = warp * J; q0 < cc.on; q0 += warps * J)
+        {
+            // ---- the owners' partner lists ----------------------------
+            int const oi = q0 + o;
+            bool const own = oi < cc.on;
+            int const t = own ? (int)order[cc.ob + oi] : cc.ob;
+            int np = 0;
+            if (own && W.d[t] < rc)
+            {
+                for (int w = wb; w < we; ++w)
+                {
+                    unsigned const mk = rangeMask(W.bits[t * words + w], w,
+                                                  cc.pb, cc.pe);
+                    for (int bit = x; bit < 32; bit += NS)
+                        if ((mk >> bit) & 1u)
+                            myList[np + __popc(mk & ((1u << bit) - 1u))] =
+                                (unsigned short)((w << 5) + bit);
+                    np += __popc(mk);
+                }
+            }
+            int most = np;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1)
+                most = max(most, __shfl_xor_sync(kFull, most, off));
+            __syncwarp();
+            // ---- steps of NS partners per owner -----------------------
+            R aG[kLockRuns], aQ[kLockRuns], aX[kLockRuns], aY[kLockRuns],
+              aZ[kLockRuns];
+#pragma unroll
+            for (int a = 0; a < kLockRuns; ++a)
+                aG[a] = aQ[a] = aX[a] = aY[a] = aZ[a] = R(0);
+            for (int p0 = 0; p0 < most; p0 += NS)
+            {
+                int const pi = p0 + x;
+                if (pi < np)
+                    stagedRecord<R, CT, NS>(P, g, C, nr, series, pow16, t,
+                                            myList[pi], W, myRec);
+                else
+                {
+#pragma unroll
+                    for (int a = 0; a < kLockRuns; ++a)
+                        myRec[3 + 3 * NS + a] = R(0);
+                }
+                __syncwarp();
+#pragma unroll
+                for (int j = 0; j < NS; ++j)
+                {
+                    R const* q = recs + (o * NS + j) * NF;
+                    R const be = q[3 + 3 * x];
+                    R const al = q[4 + 3 * x];
+                    R const ga = q[5 + 3 * x];
+                    R const rx = q[0], ry = q[1], rz = q[2];
+#pragma unroll
+                    for (int a = 0; a < kLockRuns; ++a)
+                    {
+                        R const v = q[3 + 3 * NS + a];
+                        aG[a] += v * be;
+                        aQ[a] += v * (al - eta4[a] * be);
+                        R const p3 = v * (ga + eta2[a] * be);
+                        aX[a] += p3 * rx;
+                        aY[a] += p3 * ry;
+                        aZ[a] += p3 * rz;
+                    }
+                }
+                __syncwarp();
+            }
+            // ---- slots of the group's owners; G over the owners -------
+#pragma unroll
+            for (int a = 0; a < kLockRuns; ++a)
+            {
+                if (a >= nr) break;
+                DevMember const& mm = M[g.mbeg + a * NS + x];
+                if (own && derivatives)
+                {
+                    R const fn = R(mm.factorNorm);
+                    R* const o3 = out + (long)mm.slot[cc.et] * 3 * cnt + t;
+                    o3[0] = -(fn * (aQ[a] * W.dx[t] + aX[a]));
+                    o3[cnt] = -(fn * (aQ[a] * W.dy[t] + aY[a]));
+                    o3[2 * cnt] = -(fn * (aQ[a] * W.dz[t] + aZ[a]));
+                }
+                R gs = aG[a];
+#pragma unroll
+                for (int off = NS; off < 32; off <<= 1)
+                    gs += __shfl_xor_sync(kFull, gs, off);
+                if (o == 0) W.wpG[mm.sf] += R(0.5) * gs;
+            }
+            __syncwarp();
+        }
+    }
+}
+
 template <typename R, int CT, int NS>
 __global__ void __launch_bounds__(kStagedThreads, 4)
 sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
@@ -463,6 +637,17 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     StagedCat<R, NS>* const cp = reinterpret_cast<StagedCat<R, NS>*>(cpp);
     R* const recs = reinterpret_cast<R*>(
         cpp + align16((long)sizeof(StagedCat<R, NS>)));
+    unsigned short* const plist = reinterpret_cast<unsigned short*>(
+        reinterpret_cast<char*>(recs)
+        + align16((long)sizeof(R) * stagedStride(NS) * rb));
+    unsigned short* const order = plist + (32 / NS) * cap;
+    int* const hist = reinterpret_cast<int*>(
+        reinterpret_cast<char*>(plist)
+        + align16(2L * (32 / NS) * cap + 2L * cap));
+    // The lockstep path writes only the runs' values of padding records:
+    // every record starts finite.
+    for (int k = lane; k < 32 * stagedStride(NS); k += 32) recs[k] = R(0);
+    __syncwarp();
     R* const outG = static_cast<R*>(L.G);
     R* const outNbr = static_cast<R*>(L.dGdr);
     int const numElements = P.numElements;
@@ -573,9 +758,22 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                                                 out, L.derivatives, 32 * warp,
                                                 32 * kStagedWarps);
             else if (h.type == 3 && h.shapes == NS)
-                stagedNarrow<R, CT, NS>(P, sG, sM, g0, g1, eb, cnt, words, cap,
-                                        W, list, bT, bOff, cp, recs, rb, warp,
-                                        kStagedWarps, out, L.derivatives);
+            {
+                int runs = 0;
+                for (int gi = g0; gi < g1; ++gi)
+                    runs = max(runs, sG[gi].mcnt / NS);
+                if (L.lockstep && runs <= kLockRuns)
+                    stagedNarrowLock<R, CT, NS>(P, sG, sM, g0, g1, eb, cnt,
+                                                words, cap, W, cp, recs,
+                                                plist, order, hist, warp,
+                                                kStagedWarps, out,
+                                                L.derivatives);
+                else
+                    stagedNarrow<R, CT, NS>(P, sG, sM, g0, g1, eb, cnt, words,
+                                            cap, W, list, bT, bOff, cp, recs,
+                                            rb, warp, kStagedWarps, out,
+                                            L.derivatives);
+            }
             else if (tid == 0)
                 atomicOr(&L.status[ST_FLAGS], FLAG_SF_PATH);
             __syncthreads();
