@@ -112,13 +112,13 @@ int sfDefaultVariant(SFParams const& P, int precision)
         if (P.groups[g].shapes == 4) ++n4;
         if (P.groups[g].shapes == 8) ++n8;
     }
-    // Measured on the 24,576-atom water box: the staged-triplet kernel is
-    // fastest for 8 shapes in both precisions and for 4 shapes in FP64; the
-    // software-pipelined per-owner kernel (variant 4) for 4 shapes in FP32.
-    // Potentials the staged kernel does not serve fall back to the
-    // per-owner kernels (0 in FP64; 5 with 8 shapes).
-    if (n8 > n4) return 7;
-    return precision == PREC_FP64 ? 6 : 4;
+    // Measured on the 24,576-atom water box: the staged-triplet kernel with
+    // its lockstep path is the fastest in both precisions (4 shapes in FP32:
+    // level with the software-pipelined per-owner kernel, variant 4).
+    // Potentials the staged kernel does not serve fall back to the per-owner
+    // kernels (0 with 4 shapes; 5 with 8).
+    (void)precision;
+    return n8 > n4 ? 7 : 6;
 }
 
 int sfDefaultSort(SFParams const& P)

@@ -419,7 +419,10 @@ constexpr int kLockRuns = 3;
 // word).  Records of partners beyond an owner's count carry v = 0.  The
 // owners of a category are taken in the order of their partner counts
 // (descending; buildOwnerOrder), so that a group's owners need about the
-// same number of steps.
+// same number of steps.  The groups of the segment's categories, heaviest
+// first within a category, are dealt to the warps in snake order (0 .. w-1,
+// w-1 .. 0, ...) continued across the categories, which evens out the
+// warps' work before the CTA's barrier at the segment's end.
 template <typename R, int CT, int NS>
 __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
                                  DevMember const* M, int g0, int g1,
@@ -440,9 +443,22 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
     R* const myRec = recs + lane * NF;
     int ncat = 0;
     buildCats(G, g0, g1, eb, false, 0, W, ncat);
+    int dealt = 0;   // groups dealt so far in this segment
     for (int c = 0; c < ncat; ++c)
     {
         Cat const cc = W.cats[c];
+        int const ng = (cc.on + J - 1) / J;
+        int const first = dealt;
+        dealt += ng;
+        // Does this warp get any of the category's groups?
+        bool mine = false;
+        for (int k = 0; k < ng && !mine; ++k)
+        {
+            int const pos = (first + k) % warps;
+            int const rnd = (first + k) / warps;
+            mine = ((rnd & 1) ? warps - 1 - pos : pos) == warp;
+        }
+        if (!mine) continue;
         DevGroup const& g = G[cc.gi];
         R const rc = R(g.rc);
         int const nr = g.mcnt / NS;
@@ -479,8 +495,12 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
                         hist);
         __syncwarp();
 
-        for (int q0 = warp * J; q0 < cc.on; q0 += warps * J)
+        for (int k = 0; k < ng; ++k)
         {
+            int const pos = (first + k) % warps;
+            int const rnd = (first + k) / warps;
+            if (((rnd & 1) ? warps - 1 - pos : pos) != warp) continue;
+            int const q0 = k * J;
             // ---- the owners' partner lists ----------------------------
             int const oi = q0 + o;
             bool const own = oi < cc.on;
