@@ -364,6 +364,11 @@ int n2p2b_get_stage_times(n2p2b_context* ctx, double* ms, int64_t* runs,
                           int reset);
 /* Number of kernel launches this library has issued in this process. */
 uint64_t n2p2b_kernel_launch_count(void);
+/* Diagnostics (no reference counterpart): evaluates on the current device
+ * the FP64 exponential the symmetry-function kernels use for arguments
+ * x <= 0 (y[i], i < n) and CUDA's exp (y[n + i]); x host, n values; y host,
+ * 2 n values. */
+int n2p2b_check_exp(const double* x, double* y, int64_t n);
 
 /* ---- neighbor list without memory allocation -------------------------- */
 

@@ -110,6 +110,7 @@ SIGNATURES = {
     "n2p2b_set_profiling": (C.c_int, [_vp, C.c_int]),
     "n2p2b_get_stage_times": (C.c_int, [_vp, _dp, _i64p, C.c_int]),
     "n2p2b_kernel_launch_count": (C.c_uint64, []),
+    "n2p2b_check_exp": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int64]),
     "n2p2b_neighbor_list_noalloc": (C.c_int, [
         C.c_int, _vp, C.c_int64, _vp, _vp, C.c_double, _vp, _vp, _vp, _vp,
         _vp, C.c_int64, _i64p, C.c_char_p, C.c_size_t]),

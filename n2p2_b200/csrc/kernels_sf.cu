@@ -181,4 +181,46 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,
     }
 }
 
+namespace
+{
+
+__global__ void checkExpKernel(double const* x, double* y, long n)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
+         i += (long)gridDim.x * blockDim.x)
+    {
+        y[i] = sfk::expNonPositive(x[i]);
+        y[n + i] = exp(x[i]);
+    }
+}
+
+} // namespace
+
 } // namespace n2p2b
+
+extern "C" int n2p2b_check_exp(double const* x, double* y, int64_t n)
+{
+    using namespace n2p2b;
+    if (n <= 0) return 0;
+    double* dx = nullptr;
+    double* dy = nullptr;
+    if (cudaMalloc(&dx, sizeof(double) * n) != cudaSuccess) return -3;
+    if (cudaMalloc(&dy, sizeof(double) * 2 * n) != cudaSuccess)
+    {
+        cudaFree(dx);
+        return -3;
+    }
+    cudaError_t e = cudaMemcpy(dx, x, sizeof(double) * n,
+                               cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+    {
+        noteLaunches(1);
+        checkExpKernel<<<256, 256>>>(dx, dy, (long)n);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(y, dy, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    cudaFree(dy);
+    return e == cudaSuccess ? 0 : -3;   // N2P2B_ERR_CUDA
+}

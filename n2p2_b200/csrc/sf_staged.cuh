@@ -164,13 +164,49 @@ inline bool stagedTablesShared(SFParams const& P, int cap, int ns)
         && stagedSharedBytes<R>(P, cap, ns, 32, true) <= stagedTargetBytes();
 }
 
+// exp(x) for x <= 0 in FP64 without branches: Cody and Waite's reduction
+// x = k ln2 + r, |r| <= ln2 / 2 (ln2 split into a 40-bit head, exact in
+// k ln2_hi for |k| < 2^13, and a tail), exp(r) by its Taylor polynomial of
+// degree 13 (truncation below 5e-18 relative), times 2^k assembled in the
+// exponent field.  Arguments below -708.39 (k < -1022) return 0 where libm
+// returns subnormals (< 2.3e-308).
+__device__ __forceinline__ double expNonPositive(double x)
+{
+    constexpr double kLog2e = 1.4426950408889634;
+    constexpr double kLn2Hi = 0x1.62e42fefa2000p-1;
+    constexpr double kLn2Lo = 0x1.9ef35793c7673p-41;
+    constexpr double kShift = 0x1.8p52;
+    double const t = fma(x, kLog2e, kShift);
+    int const k = __double2loint(t);
+    double const kd = t - kShift;
+    double r = fma(-kd, kLn2Hi, x);
+    r = fma(-kd, kLn2Lo, r);
+    double p = InvFact<13>::value;
+    p = fma(p, r, InvFact<12>::value);
+    p = fma(p, r, InvFact<11>::value);
+    p = fma(p, r, InvFact<10>::value);
+    p = fma(p, r, InvFact<9>::value);
+    p = fma(p, r, InvFact<8>::value);
+    p = fma(p, r, InvFact<7>::value);
+    p = fma(p, r, InvFact<6>::value);
+    p = fma(p, r, InvFact<5>::value);
+    p = fma(p, r, InvFact<4>::value);
+    p = fma(p, r, InvFact<3>::value);
+    p = fma(p, r, InvFact<2>::value);
+    p = fma(p, r, 1.0);
+    p = fma(p, r, 1.0);
+    double const two = __hiloint2double((k + 1023) << 20, 0);
+    return k < -1022 ? 0.0 : p * two;
+}
+__device__ __forceinline__ float expNonPositive(float x) { return __expf(x); }
+
 // Phase 1: the record of ordered triplet (owner t, partner k) of a group
 // with constants C.
 template <typename R, int CT, int NS>
 __device__ __forceinline__ void stagedRecord(SFParams const& P,
                                              DevGroup const& g,
                                              StagedCat<R, NS> const& C,
-                                             int nr, bool series, bool pow16,
+                                             int nr, bool series,
                                              int t, int k,
                                              WarpMem<R> const& W,
                                              R* __restrict__ rec)
@@ -217,8 +253,8 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
         int const zi = C.zi[s];
         R const pl = R(1) + C.lam[s] * cost;
         R const A = (pl <= R(0)) ? R(0)
-                  : (pow16 && zi >= 1) ? powInt16(pl, zi - 1)
-                                       : powInt(pl, zi - 1);
+                  : (zi >= 1 && zi <= 16) ? powInt16(pl, zi - 1)
+                                          : powInt(pl, zi - 1);
         R const D = A * pl;
         R const Azl = A * C.zl[s];
         R const ga = Azl * X3 - D * pr3;
@@ -231,7 +267,8 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
         if (a < nr)
         {
             R const* E = W.E + C.eoff[a];
-            rec[3 + 3 * NS + a] = E[t] * E[k] * mexp(-C.eta[a] * r2);
+            rec[3 + 3 * NS + a] = E[t] * E[k]
+                                * expNonPositive(-C.eta[a] * r2);
         }
 }
 
@@ -262,7 +299,6 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
         int const mc = g.mcnt;
         int const nr = mc / NS;
         bool const series = g.cosSeries != 0;
-        bool const pow16 = g.powBits <= 4;
         if (lane == 0)
         {
             for (int s = 0; s < NS; ++s)
@@ -344,7 +380,7 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
             for (int r = lane; r < n; r += 32)
             {
                 int const e = list[r];
-                stagedRecord<R, CT, NS>(P, g, C, nr, series, pow16,
+                stagedRecord<R, CT, NS>(P, g, C, nr, series,
                                         bT[e >> 16], e & 0xffff, W,
                                         recs + (long)r * NF);
             }
@@ -463,7 +499,6 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
         R const rc = R(g.rc);
         int const nr = g.mcnt / NS;
         bool const series = g.cosSeries != 0;
-        bool const pow16 = g.powBits <= 4;
         if (lane == 0)
         {
             for (int s = 0; s < NS; ++s)
@@ -534,7 +569,7 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             {
                 int const pi = p0 + x;
                 if (pi < np)
-                    stagedRecord<R, CT, NS>(P, g, C, nr, series, pow16, t,
+                    stagedRecord<R, CT, NS>(P, g, C, nr, series, t,
                                             myList[pi], W, myRec);
                 else
                 {

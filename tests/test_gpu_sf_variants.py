@@ -93,3 +93,30 @@ def test_variant_mixed_accuracy(gpu, monkeypatch, name, variant):
     n = len(elem)
     assert abs(e1 - e0) / n <= 1e-4
     assert np.sqrt(np.mean((f1 - f0) ** 2)) <= 5e-3
+
+
+def test_fp64_exponential(gpu):
+    """The kernels' own FP64 exponential for x <= 0 (Cody-Waite reduction,
+    Taylor polynomial) against libm (numpy) and CUDA's exp: within 2 ulp
+    where the result is normal; below the smallest normal number (libm's
+    subnormal range) it stays below that number too."""
+    import ctypes
+    from n2p2_b200 import _capi
+    lib = _capi.load()
+    rng = np.random.default_rng(3)
+    x = np.concatenate([-rng.uniform(0.0, 1.0, 100000),
+                        -rng.uniform(0.0, 50.0, 100000),
+                        -rng.uniform(0.0, 750.0, 100000),
+                        -np.array([0.0, 1e-300, 1e-17, 0.5 * np.log(2.0),
+                                   np.log(2.0), 708.3, 708.4, 745.2, 800.0])])
+    y = np.empty(2 * len(x))
+    rc = lib.n2p2b_check_exp(x.ctypes.data_as(ctypes.c_void_p),
+                             y.ctypes.data_as(ctypes.c_void_p), len(x))
+    assert rc == 0
+    ours, cuda = y[:len(x)], y[len(x):]
+    ref = np.exp(x)
+    normal = ref >= np.finfo(np.float64).tiny
+    ulp = np.spacing(ref[normal])
+    assert np.max(np.abs(ours[normal] - ref[normal]) / ulp) <= 2.0
+    assert np.max(np.abs(ours[normal] - cuda[normal]) / ulp) <= 2.0
+    assert np.all(np.abs(ours[~normal]) < np.finfo(np.float64).tiny)
