@@ -200,6 +200,45 @@ __device__ __forceinline__ double expNonPositive(double x)
 }
 __device__ __forceinline__ float expNonPositive(float x) { return __expf(x); }
 
+// pow_int (libnnp/utility.cpp:292-317) for the shape exponents zeta - 1 of
+// a record's group, which are the same in every lane of the warp (a batch or
+// lockstep group holds one category): zeta = 1, 2, 4, 8, 16 as straight
+// multiplication chains in pow_int's order (bit-identical results), other
+// exponents through the branch-free powInt16 / the loop.  FP32 keeps the
+// branch-free form throughout (measured faster there: its selects are
+// single instructions).
+template <typename R>
+__device__ __forceinline__ R powShape(R x, int n)
+{
+    if (sizeof(R) == 4)
+        return (n >= 0 && n < 16) ? powInt16(x, n) : powInt(x, n);
+    switch (n)
+    {
+    case 0: return R(1);
+    case 1: return x;
+    case 3:
+    {
+        R const x2 = x * x;
+        return x * x2;
+    }
+    case 7:
+    {
+        R const x2 = x * x;
+        R const x4 = x2 * x2;
+        return (x * x2) * x4;
+    }
+    case 15:
+    {
+        R const x2 = x * x;
+        R const x4 = x2 * x2;
+        R const x8 = x4 * x4;
+        return ((x * x2) * x4) * x8;
+    }
+    default:
+        return (n >= 0 && n < 16) ? powInt16(x, n) : powInt(x, n);
+    }
+}
+
 // Phase 1: the record of ordered triplet (owner t, partner k) of a group
 // with constants C.
 template <typename R, int CT, int NS>
@@ -252,9 +291,7 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
     {
         int const zi = C.zi[s];
         R const pl = R(1) + C.lam[s] * cost;
-        R const A = (pl <= R(0)) ? R(0)
-                  : (zi >= 1 && zi <= 16) ? powInt16(pl, zi - 1)
-                                          : powInt(pl, zi - 1);
+        R const A = (pl <= R(0)) ? R(0) : powShape(pl, zi - 1);
         R const D = A * pl;
         R const Azl = A * C.zl[s];
         R const ga = Azl * X3 - D * pr3;
