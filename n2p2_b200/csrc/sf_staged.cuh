@@ -491,8 +491,8 @@ constexpr int kLockRuns = 3;
 // list built from its validity mask (lanes of the owner split each mask
 // word).  Records of partners beyond an owner's count carry v = 0.  The
 // owners of a category are taken in the order of their partner counts
-// (descending; buildOwnerOrder), so that a group's owners need about the
-// same number of steps.  The groups of the segment's categories, heaviest
+// (descending; buildOwnerOrder, one warp per category for the whole CTA),
+// so that a group's owners need about the same number of steps.  The groups of the segment's categories, heaviest
 // first within a category, are dealt to the warps in snake order (0 .. w-1,
 // w-1 .. 0, ...) continued across the categories, which evens out the
 // warps' work before the CTA's barrier at the segment's end.
@@ -503,9 +503,9 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
                                  int words, int capE, WarpMem<R> const& W,
                                  StagedCat<R, NS>* cp, R* recs,
                                  unsigned short* plist,
-                                 unsigned short* order, int* hist, int warp,
-                                 int warps, R* __restrict__ out,
-                                 int derivatives)
+                                 unsigned short* order, int* hist,
+                                 long warpStride, int warp, int warps,
+                                 R* __restrict__ out, int derivatives)
 {
     constexpr int NF = stagedStride(NS);
     constexpr int J = 32 / NS;
@@ -517,9 +517,25 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
     int ncat = 0;
     buildCats(G, g0, g1, eb, false, 0, W, ncat);
     int dealt = 0;   // groups dealt so far in this segment
-    for (int c = 0; c < ncat; ++c)
+    // Categories in chunks of `warps`: warp w orders category cb + w's
+    // owners into its own order array, which every warp of the CTA then
+    // reads (CTA barriers around each chunk; ncat is the same in every
+    // warp).
+    for (int cb = 0; cb < ncat; cb += warps)
+    {
+    if (cb + warp < ncat)
+    {
+        Cat const cs = W.cats[cb + warp];
+        buildOwnerOrder(W, words, cs.ob, cs.ob + cs.on, cs.pb, cs.pe, order,
+                        hist);
+    }
+    __syncthreads();
+    for (int c = cb; c < min(cb + warps, ncat); ++c)
     {
         Cat const cc = W.cats[c];
+        unsigned short const* const ord = reinterpret_cast<unsigned short*>(
+            reinterpret_cast<char*>(order) + (long)(c - cb - warp)
+                                             * warpStride);
         int const ng = (cc.on + J - 1) / J;
         int const first = dealt;
         dealt += ng;
@@ -563,9 +579,6 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
         }
         int const wb = cc.pb >> 5;
         int const we = (cc.pe + 31) >> 5;
-        buildOwnerOrder(W, words, cc.ob, cc.ob + cc.on, cc.pb, cc.pe, order,
-                        hist);
-        __syncwarp();
 
         for (int k = 0; k < ng; ++k)
         {
@@ -576,7 +589,7 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             // ---- the owners' partner lists ----------------------------
             int const oi = q0 + o;
             bool const own = oi < cc.on;
-            int const t = own ? (int)order[cc.ob + oi] : cc.ob;
+            int const t = own ? (int)ord[cc.ob + oi] : cc.ob;
             int np = 0;
             if (own && W.d[t] < rc)
             {
@@ -659,6 +672,8 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             }
             __syncwarp();
         }
+    }
+    __syncthreads();   // the orders are rewritten by the next chunk
     }
 }
 
@@ -857,7 +872,8 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
                 if (L.lockstep && runs <= kLockRuns)
                     stagedNarrowLock<R, CT, NS>(P, sG, sM, g0, g1, eb, cnt,
                                                 words, cap, W, cp, recs,
-                                                plist, order, hist, warp,
+                                                plist, order, hist,
+                                                L.warpBytes, warp,
                                                 kStagedWarps, out,
                                                 L.derivatives);
                 else
