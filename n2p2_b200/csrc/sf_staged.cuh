@@ -82,6 +82,7 @@ struct StagedCat
     R   eta[kStagedRuns];
     int zi[NS];
     int eoff[kStagedRuns];   // offset of the run's exp table in W.E
+    DevGroup grp;            // the group (its cutoff parameters)
 };
 
 // Per-warp region: G sums, categories, batch list and tables, category
@@ -554,6 +555,7 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
         bool const series = g.cosSeries != 0;
         if (lane == 0)
         {
+            cp->grp = g;
             for (int s = 0; s < NS; ++s)
             {
                 DevMember const& mm = M[g.mbeg + s];
@@ -619,7 +621,7 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             {
                 int const pi = p0 + x;
                 if (pi < np)
-                    stagedRecord<R, CT, NS>(P, g, C, nr, series, t,
+                    stagedRecord<R, CT, NS>(P, C.grp, C, nr, series, t,
                                             myList[pi], W, myRec);
                 else
                 {
@@ -677,8 +679,12 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
     }
 }
 
+// Four CTAs (16 warps) per SM; FP64 with 8 shapes is held to three by its
+// shared memory (the 92-SF potential's), and gets their registers instead
+// of spilling.
 template <typename R, int CT, int NS>
-__global__ void __launch_bounds__(kStagedThreads, 4)
+__global__ void __launch_bounds__(kStagedThreads,
+                                  (sizeof(R) == 8 && NS == 8) ? 3 : 4)
 sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 {
     extern __shared__ double smem0[];
