@@ -553,23 +553,23 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
         R const rc = R(g.rc);
         int const nr = g.mcnt / NS;
         bool const series = g.cosSeries != 0;
-        if (lane == 0)
+        // The category's constants, one field set per lane.
+        if (lane < NS)
         {
-            cp->grp = g;
-            for (int s = 0; s < NS; ++s)
-            {
-                DevMember const& mm = M[g.mbeg + s];
-                cp->lam[s] = R(mm.lambda);
-                cp->zl[s] = R(mm.zetaLambda);
-                cp->zi[s] = mm.zetaInt;
-            }
-            for (int a = 0; a < kStagedRuns; ++a)
-            {
-                DevMember const& mm = M[g.mbeg + min(a, nr - 1) * NS];
-                cp->eta[a] = R(mm.eta);
-                cp->eoff[a] = mm.expIdx * capE;
-            }
+            DevMember const& mm = M[g.mbeg + lane];
+            cp->lam[lane] = R(mm.lambda);
+            cp->zl[lane] = R(mm.zetaLambda);
+            cp->zi[lane] = mm.zetaInt;
         }
+        else if (lane < NS + kStagedRuns)
+        {
+            int const a = lane - NS;
+            DevMember const& mm = M[g.mbeg + min(a, nr - 1) * NS];
+            cp->eta[a] = R(mm.eta);
+            cp->eoff[a] = mm.expIdx * capE;
+        }
+        else if (lane == 31)
+            cp->grp = g;
         __syncwarp();
         StagedCat<R, NS> const& C = *cp;
         R eta2[kLockRuns], eta4[kLockRuns];
@@ -592,19 +592,34 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             int const oi = q0 + o;
             bool const own = oi < cc.on;
             int const t = own ? (int)ord[cc.ob + oi] : cc.ob;
+            // The owner's NS lanes take one mask word each per round; a
+            // prefix of the words' counts over those lanes places each
+            // word's partners.
+            bool const act = own && W.d[t] < rc;
             int np = 0;
-            if (own && W.d[t] < rc)
+            for (int w0 = wb; w0 < we; w0 += NS)
             {
-                for (int w = wb; w < we; ++w)
+                int const w = w0 + x;
+                unsigned mk = (act && w < we)
+                            ? rangeMask(W.bits[t * words + w], w, cc.pb,
+                                        cc.pe)
+                            : 0u;
+                int const c = __popc(mk);
+                int incl = c;
+#pragma unroll
+                for (int d = 1; d < NS; d <<= 1)
                 {
-                    unsigned const mk = rangeMask(W.bits[t * words + w], w,
-                                                  cc.pb, cc.pe);
-                    for (int bit = x; bit < 32; bit += NS)
-                        if ((mk >> bit) & 1u)
-                            myList[np + __popc(mk & ((1u << bit) - 1u))] =
-                                (unsigned short)((w << 5) + bit);
-                    np += __popc(mk);
+                    int const v = __shfl_up_sync(kFull, incl, d, NS);
+                    if (x >= d) incl += v;
                 }
+                int pos = np + incl - c;
+                while (mk)
+                {
+                    int const bit = __ffs(mk) - 1;
+                    mk &= mk - 1u;
+                    myList[pos++] = (unsigned short)((w << 5) + bit);
+                }
+                np += __shfl_sync(kFull, incl, NS - 1, NS);
             }
             int most = np;
 #pragma unroll
