@@ -186,10 +186,14 @@ namespace
 
 __global__ void checkExpKernel(double const* x, double* y, long n)
 {
+    __shared__ double tab[sfk::kExpTableSize];
+    for (int j = threadIdx.x; j < sfk::kExpTableSize; j += blockDim.x)
+        tab[j] = sfk::kExp2Table[j];
+    __syncthreads();
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n;
          i += (long)gridDim.x * blockDim.x)
     {
-        y[i] = sfk::expNonPositive(x[i]);
+        y[i] = sfk::expNonPositive(x[i], tab);
         y[n + i] = exp(x[i]);
     }
 }

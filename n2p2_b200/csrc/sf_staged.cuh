@@ -49,9 +49,10 @@ constexpr int kStagedThreads = kThreads;   // 4 warps, one atom
 constexpr int kStagedWarps = kWarps;
 // eta runs per group the records hold (groups have at most this many).
 constexpr int kStagedRuns = 4;
-// Shared memory per CTA the record capacity is sized for: four CTAs per SM
+// Dynamic shared memory per CTA the record capacity is sized for: four CTAs
+// per SM, less the exponential's table (static, 512 bytes)
 // (N2P2B_SF_STAGED_KB overrides it, in KB, for measurements).
-constexpr long kStagedTargetBytes = 56L * 1024;
+constexpr long kStagedTargetBytes = 56L * 1024 - 512;
 inline long stagedTargetBytes()
 {
     static long const v = [] {
@@ -82,6 +83,8 @@ struct StagedCat
     R   eta[kStagedRuns];
     int zi[NS];
     int eoff[kStagedRuns];   // offset of the run's exp table in W.E
+    R   a2q, qf;             // a^2 / 4 and -a^2 / 2, a = pi / rc (the
+                             // FP64 cosine cutoff's series)
     DevGroup grp;            // the group (its cutoff parameters)
 };
 
@@ -165,41 +168,70 @@ inline bool stagedTablesShared(SFParams const& P, int cap, int ns)
         && stagedSharedBytes<R>(P, cap, ns, 32, true) <= stagedTargetBytes();
 }
 
-// exp(x) for x <= 0 in FP64 without branches: Cody and Waite's reduction
-// x = k ln2 + r, |r| <= ln2 / 2 (ln2 split into a 40-bit head, exact in
-// k ln2_hi for |k| < 2^13, and a tail), exp(r) by its Taylor polynomial of
-// degree 13 (truncation below 5e-18 relative), times 2^k assembled in the
-// exponent field.  Arguments below -708.39 (k < -1022) return 0 where libm
-// returns subnormals (< 2.3e-308).
-__device__ __forceinline__ double expNonPositive(double x)
+// 2^(j / 64), j = 0 .. 63, rounded to nearest: the table of the exponential
+// below, staged into shared memory by the kernels that use it.
+static __constant__ double kExp2Table[64] = {
+    0x1.0000000000000p+0, 0x1.02c9a3e778061p+0, 0x1.059b0d3158574p+0,
+    0x1.0874518759bc8p+0, 0x1.0b5586cf9890fp+0, 0x1.0e3ec32d3d1a2p+0,
+    0x1.11301d0125b51p+0, 0x1.1429aaea92de0p+0, 0x1.172b83c7d517bp+0,
+    0x1.1a35beb6fcb75p+0, 0x1.1d4873168b9aap+0, 0x1.2063b88628cd6p+0,
+    0x1.2387a6e756238p+0, 0x1.26b4565e27cddp+0, 0x1.29e9df51fdee1p+0,
+    0x1.2d285a6e4030bp+0, 0x1.306fe0a31b715p+0, 0x1.33c08b26416ffp+0,
+    0x1.371a7373aa9cbp+0, 0x1.3a7db34e59ff7p+0, 0x1.3dea64c123422p+0,
+    0x1.4160a21f72e2ap+0, 0x1.44e086061892dp+0, 0x1.486a2b5c13cd0p+0,
+    0x1.4bfdad5362a27p+0, 0x1.4f9b2769d2ca7p+0, 0x1.5342b569d4f82p+0,
+    0x1.56f4736b527dap+0, 0x1.5ab07dd485429p+0, 0x1.5e76f15ad2148p+0,
+    0x1.6247eb03a5585p+0, 0x1.6623882552225p+0, 0x1.6a09e667f3bcdp+0,
+    0x1.6dfb23c651a2fp+0, 0x1.71f75e8ec5f74p+0, 0x1.75feb564267c9p+0,
+    0x1.7a11473eb0187p+0, 0x1.7e2f336cf4e62p+0, 0x1.82589994cce13p+0,
+    0x1.868d99b4492edp+0, 0x1.8ace5422aa0dbp+0, 0x1.8f1ae99157736p+0,
+    0x1.93737b0cdc5e5p+0, 0x1.97d829fde4e50p+0, 0x1.9c49182a3f090p+0,
+    0x1.a0c667b5de565p+0, 0x1.a5503b23e255dp+0, 0x1.a9e6b5579fdbfp+0,
+    0x1.ae89f995ad3adp+0, 0x1.b33a2b84f15fbp+0, 0x1.b7f76f2fb5e47p+0,
+    0x1.bcc1e904bc1d2p+0, 0x1.c199bdd85529cp+0, 0x1.c67f12e57d14bp+0,
+    0x1.cb720dcef9069p+0, 0x1.d072d4a07897cp+0, 0x1.d5818dcfba487p+0,
+    0x1.da9e603db3285p+0, 0x1.dfc97337b9b5fp+0, 0x1.e502ee78b3ff6p+0,
+    0x1.ea4afa2a490dap+0, 0x1.efa1bee615a27p+0, 0x1.f50765b6e4540p+0,
+    0x1.fa7c1819e90d8p+0,
+};
+constexpr int kExpTableSize = 64;
+
+// exp(x) for x <= 0 in FP64 without branches, by Tang's table-driven method
+// (P. T. P. Tang, ACM TOMS 15 (1989) 144-157): x = (64 m + j) ln2 / 64 + r,
+// |r| <= ln2 / 128, with ln2 / 64 split into a 32-bit head (k ln2_hi exact
+// for |k| < 2^21) and a tail; exp(x) = 2^m T[j] (1 + q), q = exp(r) - 1 by
+// its Taylor polynomial of degree 6 (truncation below 2.7e-20), formed as
+// T[j] + T[j] q so that q's rounding hardly counts.  Within 1.01 ulp of the
+// exact value where the result is normal.  Arguments below -708.39
+// (m < -1022) return 0 where libm returns subnormals (< 2.3e-308).  tab is
+// kExp2Table in shared memory.
+__device__ __forceinline__ double expNonPositive(double x,
+                                                 double const* tab)
 {
-    constexpr double kLog2e = 1.4426950408889634;
-    constexpr double kLn2Hi = 0x1.62e42fefa2000p-1;
-    constexpr double kLn2Lo = 0x1.9ef35793c7673p-41;
+    constexpr double kInvL = 0x1.71547652b82fep+6;     // 64 / ln2
+    constexpr double kLHi = 0x1.62e42fee00000p-7;      // ln2 / 64, head
+    constexpr double kLLo = 0x1.a39ef35793c76p-39;     // ln2 / 64, tail
     constexpr double kShift = 0x1.8p52;
-    double const t = fma(x, kLog2e, kShift);
+    double const t = fma(x, kInvL, kShift);
     int const k = __double2loint(t);
     double const kd = t - kShift;
-    double r = fma(-kd, kLn2Hi, x);
-    r = fma(-kd, kLn2Lo, r);
-    double p = InvFact<13>::value;
-    p = fma(p, r, InvFact<12>::value);
-    p = fma(p, r, InvFact<11>::value);
-    p = fma(p, r, InvFact<10>::value);
-    p = fma(p, r, InvFact<9>::value);
-    p = fma(p, r, InvFact<8>::value);
-    p = fma(p, r, InvFact<7>::value);
-    p = fma(p, r, InvFact<6>::value);
-    p = fma(p, r, InvFact<5>::value);
+    double r = fma(-kd, kLHi, x);
+    r = fma(-kd, kLLo, r);
+    double const r2 = r * r;
+    double p = fma(r, InvFact<6>::value, InvFact<5>::value);
     p = fma(p, r, InvFact<4>::value);
     p = fma(p, r, InvFact<3>::value);
-    p = fma(p, r, InvFact<2>::value);
-    p = fma(p, r, 1.0);
-    p = fma(p, r, 1.0);
-    double const two = __hiloint2double((k + 1023) << 20, 0);
-    return k < -1022 ? 0.0 : p * two;
+    p = fma(p, r, 0.5);
+    double const q = fma(p, r2, r);
+    double const tj = tab[k & (kExpTableSize - 1)];
+    int const m = k >> 6;
+    double const two = __hiloint2double((m + 1023) << 20, 0);
+    return m < -1022 ? 0.0 : fma(tj, q, tj) * two;
 }
-__device__ __forceinline__ float expNonPositive(float x) { return __expf(x); }
+__device__ __forceinline__ float expNonPositive(float x, double const*)
+{
+    return __expf(x);
+}
 
 // pow_int (libnnp/utility.cpp:292-317) for the shape exponents zeta - 1 of
 // a record's group, which are the same in every lane of the warp (a batch or
@@ -262,15 +294,15 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
     R const cost = (dr1[0] * dr2[0] + dr1[1] * dr2[1] + dr1[2] * dr2[2])
                  * rinvijik;
     R const r2 = dr3[0] * dr3[0] + dr3[1] * dr3[1] + dr3[2] * dr3[2];
-    // f_c(r_jk) and f_c'(r_jk) / r_jk (FP64 cosine cutoff: power series in
-    // r_jk^2, see cosSincSeries).
+    // f_c(r_jk) and f_c'(r_jk) / r_jk (FP64 cosine cutoff: half-angle power
+    // series in r_jk^2, see halfAngleCosSinc).
     R pfcjk, qjk;
     if ((sizeof(R) == 8) && (CT == 1) && series)
     {
-        double c, sc;
-        cosSincSeries((double)(R(g.a2) * r2), c, sc);
-        pfcjk = R(0.5) * R(c) + R(0.5);
-        qjk = R(-0.5) * R(g.a2) * R(sc);
+        double ch, sh;
+        halfAngleCosSinc((double)(C.a2q * r2), ch, sh);
+        pfcjk = R(ch * ch);
+        qjk = C.qf * R(sh * ch);
     }
     else
     {
@@ -279,10 +311,15 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
         cutoffFdf<R, CT>(P, g, r2 * invjk, pfcjk, pdfcjk);
         qjk = pdfcjk * invjk;
     }
-    R const pfc = pfcij * pfcik * pfcjk;
+    // alpha' = A (zl X1 + plambda pr1) - gamma with gamma = A (zl X3 -
+    // plambda pr3) is A zl (X1 - X3) + D (pr1 + pr3), D = A plambda, and
+    // X1 - X3 = -pfc cos / r_ij^2.
+    R const fijik = pfcij * pfcik;
+    R const pfc = fijik * pfcjk;
     R const pr1 = pfcik * pfcjk * pdfcrij;
-    R const pr3 = pfcij * pfcik * qjk;
-    R const X1 = pfc * (rinvijik - cost * (invij * invij));
+    R const pr3 = fijik * qjk;
+    R const pr13 = pr1 + pr3;
+    R const Xc = -(pfc * cost) * (invij * invij);
     R const X3 = pfc * rinvijik;
     rec[0] = dr2[0];
     rec[1] = dr2[1];
@@ -295,10 +332,9 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
         R const A = (pl <= R(0)) ? R(0) : powShape(pl, zi - 1);
         R const D = A * pl;
         R const Azl = A * C.zl[s];
-        R const ga = Azl * X3 - D * pr3;
         rec[3 + 3 * s] = D * pfc;
-        rec[4 + 3 * s] = (Azl * X1 + D * pr1) - ga;
-        rec[5 + 3 * s] = ga;
+        rec[4 + 3 * s] = Azl * Xc + D * pr13;
+        rec[5 + 3 * s] = Azl * X3 - D * pr3;
     }
 #pragma unroll
     for (int a = 0; a < kStagedRuns; ++a)
@@ -306,7 +342,7 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
         {
             R const* E = W.E + C.eoff[a];
             rec[3 + 3 * NS + a] = E[t] * E[k]
-                                * expNonPositive(-C.eta[a] * r2);
+                                * expNonPositive(-C.eta[a] * r2, W.expTab);
         }
 }
 
@@ -352,6 +388,8 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
                 cp->eta[a] = R(mm.eta);
                 cp->eoff[a] = mm.expIdx * capE;
             }
+            cp->a2q = R(0.25) * R(g.a2);
+            cp->qf = R(-0.5) * R(g.a2);
         }
         // Phase-2 lane: member m of slice s (S slices of the partners).
         int const S = 32 / mc;
@@ -569,7 +607,11 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             cp->eoff[a] = mm.expIdx * capE;
         }
         else if (lane == 31)
+        {
             cp->grp = g;
+            cp->a2q = R(0.25) * R(g.a2);
+            cp->qf = R(-0.5) * R(g.a2);
+        }
         __syncwarp();
         StagedCat<R, NS> const& C = *cp;
         R eta2[kLockRuns], eta4[kLockRuns];
@@ -658,7 +700,7 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
                     {
                         R const v = q[3 + 3 * NS + a];
                         aG[a] += v * be;
-                        aQ[a] += v * (al - eta4[a] * be);
+                        aQ[a] += v * al;
                         R const p3 = v * (ga + eta2[a] * be);
                         aX[a] += p3 * rx;
                         aY[a] += p3 * ry;
@@ -675,11 +717,14 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
                 DevMember const& mm = M[g.mbeg + a * NS + x];
                 if (own && derivatives)
                 {
+                    // Q = sum v (alpha' - 4 eta beta) = sum v alpha'
+                    //     - 4 eta G.
                     R const fn = R(mm.factorNorm);
+                    R const Q = aQ[a] - eta4[a] * aG[a];
                     R* const o3 = out + (long)mm.slot[cc.et] * 3 * cnt + t;
-                    o3[0] = -(fn * (aQ[a] * W.dx[t] + aX[a]));
-                    o3[cnt] = -(fn * (aQ[a] * W.dy[t] + aY[a]));
-                    o3[2 * cnt] = -(fn * (aQ[a] * W.dz[t] + aZ[a]));
+                    o3[0] = -(fn * (Q * W.dx[t] + aX[a]));
+                    o3[cnt] = -(fn * (Q * W.dy[t] + aY[a]));
+                    o3[2 * cnt] = -(fn * (Q * W.dz[t] + aZ[a]));
                 }
                 R gs = aG[a];
 #pragma unroll
@@ -703,9 +748,13 @@ __global__ void __launch_bounds__(kStagedThreads,
 sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
 {
     extern __shared__ double smem0[];
+    __shared__ double expTab[sizeof(R) == 8 ? kExpTableSize : 1];
     int const ng = P.numGroups;
     int const nm = P.numMembers;
     int const tid = threadIdx.x;
+    if (sizeof(R) == 8)
+        for (int j = tid; j < kExpTableSize; j += kStagedThreads)
+            expTab[j] = kExp2Table[j];
     // Group and member tables: staged in shared memory when they fit the
     // CTA's budget, else read from global memory through L1.
     bool const tables = L.tablesShared != 0;
@@ -748,6 +797,7 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
     W.E = W.dfcr + cap;
     W.bits = reinterpret_cast<unsigned*>(
         base + align16((long)sizeof(R) * (7L + P.maxExp) * cap));
+    W.expTab = expTab;
     char* const warps0 = base + stagedAtomBytes<R>(P.maxExp, cap);
     char* const wp = warps0 + (long)warp * L.warpBytes;
     W.wpG = reinterpret_cast<R*>(wp);

@@ -105,3 +105,32 @@ int main(int argc, char** argv)
                         "-L" + lib, "-ln2p2b200"],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_exponential_table_is_correctly_rounded():
+    """The FP64 exponential of the staged symmetry-function kernel reads
+    2^(j / 64), j = 0 .. 63, from a table in sf_staged.cuh; every entry is
+    the double nearest to the exact value (checked at 200 bits), and the
+    reduction constants are ln2 / 64 split into a 32-bit head and its
+    tail, and 64 / ln2 rounded."""
+    mpmath = pytest.importorskip("mpmath")
+    src = os.path.join(os.path.dirname(__file__), "..", "n2p2_b200", "csrc",
+                       "sf_staged.cuh")
+    text = open(src).read()
+    body = text[text.index("kExp2Table[64] = {"):]
+    body = body[:body.index("};")]
+    vals = [float.fromhex(h) for h in re.findall(r"0x[0-9a-f.]+p[+-]\d+",
+                                                 body)]
+    assert len(vals) == 64
+    mpmath.mp.prec = 200
+    for j, v in enumerate(vals):
+        exact = mpmath.power(2, mpmath.mpf(j) / 64)
+        assert v == float(exact)
+    consts = dict(re.findall(r"constexpr double (k\w+) = (0x[0-9a-f.]+p[+-]\d+)",
+                             text))
+    hi = float.fromhex(consts["kLHi"])
+    lo = float.fromhex(consts["kLLo"])
+    ln2_64 = mpmath.log(2) / 64
+    assert float(64 / mpmath.log(2)) == float.fromhex(consts["kInvL"])
+    assert int(mpmath.mpf(hi) * 2 ** 38) == mpmath.mpf(hi) * 2 ** 38
+    assert lo == float(ln2_64 - mpmath.mpf(hi))
