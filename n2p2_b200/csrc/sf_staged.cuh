@@ -513,6 +513,81 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
     }
 }
 
+// Radial groups (SymGrpExpRad, libnnp/SymGrpExpRad.cpp:144-239, and the
+// element-weighted type 12) of segment [g0, g1).  Per category (group,
+// neighbor element) lane (member m, sub-lane u) of warp w takes neighbors
+// ob + w S + u, ob + (w + warps) S + u, ... (S = 32 / members sub-lanes),
+// writes the member's slot of each and sums its G terms in that order; the
+// S sums of a member are then added by a fixed tree and the member's G
+// gets the total once per category.  Neighbors beyond the group's cutoff
+// get zero slots.
+template <typename R>
+__device__ void stagedRadial(SFParams const& P, DevGroup const* G,
+                             DevMember const* M, int g0, int g1,
+                             int const eb[kMaxElem + 1], int cnt,
+                             WarpMem<R> const& W, R* __restrict__ out,
+                             int derivatives, int warp, int warps)
+{
+    int const lane = threadIdx.x & 31;
+    for (int gi = g0; gi < g1; ++gi)
+    {
+        DevGroup const& g = G[gi];
+        bool const weighted = g.type == 12;
+        R const rc = R(g.rc);
+        for (int et = 0; et < kMaxElem; ++et)
+        {
+            int const ob = eb[et], oe = eb[et + 1];
+            if (weighted ? (oe <= ob) : (et != g.e1)) continue;
+            R const z = weighted ? R(P.atomicNumber[et]) : R(1);
+            for (int mb = 0; mb < g.mcnt; mb += 32)
+            {
+                int const mn = min(32, g.mcnt - mb);
+                int const S = 32 / mn;
+                int const u = lane / mn;
+                int const m = mb + lane - u * mn;
+                bool const act = u < S;
+                DevMember const& mm = M[g.mbeg + (act ? m : mb)];
+                R const eta = R(mm.eta), rs = R(mm.rs);
+                R const fn = R(mm.factorNorm);
+                R* const o3 = out + (long)mm.slot[et] * 3 * cnt;
+                R gs = R(0);
+                if (act)
+                    for (int t = ob + warp * S + u; t < oe; t += warps * S)
+                    {
+                        R const r = W.d[t];
+                        R p1 = R(0);
+                        if (r < rc)
+                        {
+                            // SymGrpExpRad.cpp:210-211 with (f_c' - 2 eta
+                            // (r - rs) f_c) / r written as f_c' / r - 2 eta
+                            // (r - rs) f_c / r.
+                            R const rr = r - rs;
+                            R const pfc = W.fc[t];
+                            R const pexp = z * expNonPositive(-eta * rr * rr,
+                                                              W.expTab);
+                            gs += pexp * pfc;
+                            p1 = fn * (W.dfcr[t] - R(2) * eta * rr * pfc
+                                                   * W.inv[t]) * pexp;
+                        }
+                        if (derivatives)
+                        {
+                            o3[t] = -(p1 * W.dx[t]);
+                            o3[cnt + t] = -(p1 * W.dy[t]);
+                            o3[2 * cnt + t] = -(p1 * W.dz[t]);
+                        }
+                    }
+                for (int d = 1; d < S; d <<= 1)
+                {
+                    R const v = __shfl_down_sync(kFull, gs, d * mn);
+                    if ((u & (2 * d - 1)) == 0 && u + d < S) gs += v;
+                }
+                if (u == 0) W.wpG[mm.sf] += gs;
+                __syncwarp();
+            }
+        }
+    }
+}
+
 // Eta runs per group the lockstep path keeps in registers.
 constexpr int kLockRuns = 3;
 
@@ -531,10 +606,11 @@ constexpr int kLockRuns = 3;
 // word).  Records of partners beyond an owner's count carry v = 0.  The
 // owners of a category are taken in the order of their partner counts
 // (descending; buildOwnerOrder, one warp per category for the whole CTA),
-// so that a group's owners need about the same number of steps.  The groups of the segment's categories, heaviest
-// first within a category, are dealt to the warps in snake order (0 .. w-1,
-// w-1 .. 0, ...) continued across the categories, which evens out the
-// warps' work before the CTA's barrier at the segment's end.
+// so that a group's owners need about the same number of steps.  The
+// groups of the segment's categories, heaviest first within a category, are
+// dealt to the warps in snake order (0 .. w-1, w-1 .. 0, ...) continued
+// across the categories, which evens out the warps' work before the CTA's
+// barrier at the segment's end.
 template <typename R, int CT, int NS>
 __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
                                  DevMember const* M, int g0, int g1,
@@ -886,25 +962,26 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             if (h.type == 3 && h.rc != bitsRc)
             {
                 // Narrow-angular validity: k != t, r_ik < rc, r_jk^2 < rc^2.
+                // Warp v takes rows t = v, v + warps, ...; lane l of word w
+                // tests partner k = 32 w + l, and the word is the ballot.
                 R const rc = R(h.rc), rc2 = R(h.rc2);
-                for (int t = tid; t < cnt; t += kStagedThreads)
+                for (int w = 0; w < words; ++w)
                 {
-                    R const x = W.dx[t], y = W.dy[t], z = W.dz[t];
-                    for (int w = 0; w < words; ++w)
+                    int const k = (w << 5) + lane;
+                    int const kk = k < cnt ? k : 0;
+                    bool const okk = (k < cnt) && (W.d[kk] < rc);
+                    R const xk = W.dx[kk];
+                    R const yk = W.dy[kk];
+                    R const zk = W.dz[kk];
+                    for (int t = warp; t < cnt; t += kStagedWarps)
                     {
-                        unsigned m = 0u;
-                        int const kb = w << 5;
-                        int const ke = min(cnt, kb + 32);
-                        for (int k = kb; k < ke; ++k)
-                        {
-                            R const a = W.dx[k] - x;
-                            R const b = W.dy[k] - y;
-                            R const c = W.dz[k] - z;
-                            bool const ok = (k != t) && (W.d[k] < rc)
-                                          && (a * a + b * b + c * c < rc2);
-                            m |= (ok ? 1u : 0u) << (k - kb);
-                        }
-                        W.bits[t * words + w] = m;
+                        R const a = xk - W.dx[t];
+                        R const b = yk - W.dy[t];
+                        R const c = zk - W.dz[t];
+                        bool const ok = okk && (k != t)
+                                      && (a * a + b * b + c * c < rc2);
+                        unsigned const m = __ballot_sync(kFull, ok);
+                        if (lane == 0) W.bits[t * words + w] = m;
                     }
                 }
                 bitsRc = h.rc;
@@ -932,9 +1009,8 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             }
             __syncthreads();
             if (h.type == 2 || h.type == 12)
-                radialSegment<R, kGenericChunk>(P, sG, sM, g0, g1, eb, cnt, W,
-                                                out, L.derivatives, 32 * warp,
-                                                32 * kStagedWarps);
+                stagedRadial<R>(P, sG, sM, g0, g1, eb, cnt, W, out,
+                                L.derivatives, warp, kStagedWarps);
             else if (h.type == 3 && h.shapes == NS)
             {
                 int runs = 0;
