@@ -272,23 +272,51 @@ __device__ __forceinline__ R powShape(R x, int n)
     }
 }
 
+// The owner's staged values a record reads (loaded once per owner).
+template <typename R>
+struct StagedOwner
+{
+    R dr[3], inv, fc, dfcr;
+    R E[kStagedRuns];   // E_a(r_ij) of the group's eta runs
+};
+
+template <typename R, int NS>
+__device__ __forceinline__ StagedOwner<R> stagedOwner(WarpMem<R> const& W,
+                                                      StagedCat<R, NS> const& C,
+                                                      int nr, int t)
+{
+    StagedOwner<R> v;
+    v.dr[0] = W.dx[t];
+    v.dr[1] = W.dy[t];
+    v.dr[2] = W.dz[t];
+    v.inv = W.inv[t];
+    v.fc = W.fc[t];
+    v.dfcr = W.dfcr[t];
+#pragma unroll
+    for (int a = 0; a < kStagedRuns; ++a)
+        v.E[a] = (a < nr) ? W.E[C.eoff[a] + t] : R(0);
+    return v;
+}
+
 // Phase 1: the record of ordered triplet (owner t, partner k) of a group
-// with constants C.
-template <typename R, int CT, int NS>
+// with constants C; HOIST: the owner's values come from ow (else they are
+// read from the staged arrays here).
+template <typename R, int CT, int NS, bool HOIST>
 __device__ __forceinline__ void stagedRecord(SFParams const& P,
                                              DevGroup const& g,
                                              StagedCat<R, NS> const& C,
-                                             int nr, bool series,
-                                             int t, int k,
+                                             int nr, bool series, int t,
+                                             StagedOwner<R> const& ow, int k,
                                              WarpMem<R> const& W,
                                              R* __restrict__ rec)
 {
-    R const dr1[3] = {W.dx[t], W.dy[t], W.dz[t]};
+    R const dr1[3] = {HOIST ? ow.dr[0] : W.dx[t], HOIST ? ow.dr[1] : W.dy[t],
+                      HOIST ? ow.dr[2] : W.dz[t]};
     R const dr2[3] = {W.dx[k], W.dy[k], W.dz[k]};
-    R const invij = W.inv[t];
-    R const pfcij = W.fc[t];
+    R const invij = HOIST ? ow.inv : W.inv[t];
+    R const pfcij = HOIST ? ow.fc : W.fc[t];
     R const pfcik = W.fc[k];
-    R const pdfcrij = W.dfcr[t];
+    R const pdfcrij = HOIST ? ow.dfcr : W.dfcr[t];
     R const dr3[3] = {dr2[0] - dr1[0], dr2[1] - dr1[1], dr2[2] - dr1[2]};
     R const rinvijik = invij * W.inv[k];
     R const cost = (dr1[0] * dr2[0] + dr1[1] * dr2[1] + dr1[2] * dr2[2])
@@ -341,7 +369,7 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
         if (a < nr)
         {
             R const* E = W.E + C.eoff[a];
-            rec[3 + 3 * NS + a] = E[t] * E[k]
+            rec[3 + 3 * NS + a] = (HOIST ? ow.E[a] : E[t]) * E[k]
                                 * expNonPositive(-C.eta[a] * r2, W.expTab);
         }
 }
@@ -456,9 +484,10 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
             for (int r = lane; r < n; r += 32)
             {
                 int const e = list[r];
-                stagedRecord<R, CT, NS>(P, g, C, nr, series,
-                                        bT[e >> 16], e & 0xffff, W,
-                                        recs + (long)r * NF);
+                stagedRecord<R, CT, NS, false>(P, g, C, nr, series,
+                                               bT[e >> 16], StagedOwner<R>(),
+                                               e & 0xffff, W,
+                                               recs + (long)r * NF);
             }
             __syncwarp();
             // ---- phase 2: lanes (member, slice) over each owner ---------
@@ -714,6 +743,12 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             // prefix of the words' counts over those lanes places each
             // word's partners.
             bool const act = own && W.d[t] < rc;
+            // The owner's values stay in registers for the group where
+            // they fit (8 shapes: 3 CTAs per SM); with 4 shapes they are
+            // read per record, which keeps 4 CTAs per SM without spills.
+            constexpr bool kHoist = NS == 8;
+            StagedOwner<R> ow{};
+            if constexpr (kHoist) ow = stagedOwner(W, C, nr, t);
             int np = 0;
             for (int w0 = wb; w0 < we; w0 += NS)
             {
@@ -754,8 +789,9 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
             {
                 int const pi = p0 + x;
                 if (pi < np)
-                    stagedRecord<R, CT, NS>(P, C.grp, C, nr, series, t,
-                                            myList[pi], W, myRec);
+                    stagedRecord<R, CT, NS, kHoist>(P, C.grp, C, nr, series,
+                                                    t, ow, myList[pi], W,
+                                                    myRec);
                 else
                 {
 #pragma unroll
@@ -962,26 +998,46 @@ sfStagedKernel(__grid_constant__ SFParams const P, SFLaunch const L)
             if (h.type == 3 && h.rc != bitsRc)
             {
                 // Narrow-angular validity: k != t, r_ik < rc, r_jk^2 < rc^2.
-                // Warp v takes rows t = v, v + warps, ...; lane l of word w
-                // tests partner k = 32 w + l, and the word is the ballot.
+                // Warp v takes rows t = v, v + warps, ...; lane l holds the
+                // partners k = 32 w + l of four words at a time, and each
+                // word is a ballot (only the words holding partners,
+                // ceil(cnt / 32), are formed; no one reads the others).
                 R const rc = R(h.rc), rc2 = R(h.rc2);
-                for (int w = 0; w < words; ++w)
+                int const wn = (cnt + 31) >> 5;
+                for (int w0 = 0; w0 < wn; w0 += 4)
                 {
-                    int const k = (w << 5) + lane;
-                    int const kk = k < cnt ? k : 0;
-                    bool const okk = (k < cnt) && (W.d[kk] < rc);
-                    R const xk = W.dx[kk];
-                    R const yk = W.dy[kk];
-                    R const zk = W.dz[kk];
+                    R xk[4], yk[4], zk[4];
+                    bool okk[4];
+#pragma unroll
+                    for (int j = 0; j < 4; ++j)
+                    {
+                        int const k = ((w0 + j) << 5) + lane;
+                        int const kk = k < cnt ? k : 0;
+                        okk[j] = (k < cnt) && (W.d[kk] < rc);
+                        xk[j] = W.dx[kk];
+                        yk[j] = W.dy[kk];
+                        zk[j] = W.dz[kk];
+                    }
                     for (int t = warp; t < cnt; t += kStagedWarps)
                     {
-                        R const a = xk - W.dx[t];
-                        R const b = yk - W.dy[t];
-                        R const c = zk - W.dz[t];
-                        bool const ok = okk && (k != t)
-                                      && (a * a + b * b + c * c < rc2);
-                        unsigned const m = __ballot_sync(kFull, ok);
-                        if (lane == 0) W.bits[t * words + w] = m;
+                        R const xt = W.dx[t], yt = W.dy[t], zt = W.dz[t];
+                        unsigned m[4];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                        {
+                            R const a = xk[j] - xt;
+                            R const b = yk[j] - yt;
+                            R const c = zk[j] - zt;
+                            bool const ok = okk[j]
+                                          && (((w0 + j) << 5) + lane != t)
+                                          && (a * a + b * b + c * c < rc2);
+                            m[j] = __ballot_sync(kFull, ok);
+                        }
+                        unsigned const mine = lane == 0 ? m[0]
+                                            : lane == 1 ? m[1]
+                                            : lane == 2 ? m[2] : m[3];
+                        if (lane < min(4, wn - w0))
+                            W.bits[t * words + w0 + lane] = mine;
                     }
                 }
                 bitsRc = h.rc;
