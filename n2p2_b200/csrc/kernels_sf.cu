@@ -150,12 +150,9 @@ void launchSymmetryFunctions(SFParams const& P, SFLaunch const& L0,
         L.recCap = g.rb;
         L.tablesShared = g.tables ? 1 : 0;
         // N2P2B_SF_LOCKSTEP=0 keeps the batched (member, slice) path for
-        // every narrow segment (measurements).
-        static int const lock = [] {
-            char const* e = std::getenv("N2P2B_SF_LOCKSTEP");
-            return e ? std::atoi(e) : 1;
-        }();
-        L.lockstep = lock;
+        // every narrow segment (measurements, tests; read per launch).
+        char const* lockEnv = std::getenv("N2P2B_SF_LOCKSTEP");
+        L.lockstep = lockEnv ? std::atoi(lockEnv) : 1;
         L.warpBytes = g.warpBytes;
         shm = g.shm;
     }

@@ -46,7 +46,20 @@ def _models(name, variant, monkeypatch, precision="fp64"):
 @pytest.mark.parametrize("variant", VARIANTS)
 @pytest.mark.parametrize("name", ["h2o_52", "h2o_92"])
 def test_variant_intermediates(gpu, monkeypatch, name, variant):
-    p, ref = _models(name, variant, monkeypatch)
+    _check_intermediates(*_models(name, variant, monkeypatch))
+
+
+@pytest.mark.parametrize("variant", [6, 7])
+@pytest.mark.parametrize("name", ["h2o_52", "h2o_92"])
+def test_staged_batched_path(gpu, monkeypatch, name, variant):
+    """The staged kernel's batched path (owners in batches, lanes over
+    (member, partner slice)), which serves groups of four eta runs, forced
+    for every narrow group by N2P2B_SF_LOCKSTEP=0."""
+    monkeypatch.setenv("N2P2B_SF_LOCKSTEP", "0")
+    _check_intermediates(*_models(name, variant, monkeypatch))
+
+
+def _check_intermediates(p, ref):
     box, pos, elem = synth.water_box(64, 3)
     ref.set_structure(pos, elem, box)
     ref.evaluate(True)
