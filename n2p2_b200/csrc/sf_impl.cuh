@@ -686,6 +686,10 @@ __device__ __forceinline__ unsigned rangeMask(unsigned m, int w, int pb,
 // sorted by their number of valid partners, descending, by a stable warp
 // counting sort over 32 buckets of the count range (exact when the counts
 // span at most 32 values). Writes order[ob .. oe). Warp-uniform arguments.
+// The counts of the first kOrderCached rounds of 32 owners are kept in
+// registers across the three passes (min / max, histogram, placement);
+// later rounds count again.
+constexpr int kOrderCached = 4;
 template <typename R>
 __device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
                                 int oe, int pb, int pe,
@@ -700,8 +704,20 @@ __device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
             c += __popc(rangeMask(W.bits[t * words + w], w, pb, pe));
         return c;
     };
+    int cc[kOrderCached];
     int cmin = 0x7fffffff, cmax = 0;
-    for (int t = ob + lane; t < oe; t += 32)
+#pragma unroll
+    for (int r = 0; r < kOrderCached; ++r)
+    {
+        int const t = ob + 32 * r + lane;
+        cc[r] = (t < oe) ? count(t) : 0;
+        if (t < oe)
+        {
+            cmin = min(cmin, cc[r]);
+            cmax = max(cmax, cc[r]);
+        }
+    }
+    for (int t = ob + 32 * kOrderCached + lane; t < oe; t += 32)
     {
         int const c = count(t);
         cmin = min(cmin, c);
@@ -717,7 +733,10 @@ __device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
     auto key = [&](int c) { return ((cmax - c) * 32) / span; };
     hist[lane] = 0;
     __syncwarp();
-    for (int t = ob + lane; t < oe; t += 32)
+#pragma unroll
+    for (int r = 0; r < kOrderCached; ++r)
+        if (ob + 32 * r + lane < oe) atomicAdd(&hist[key(cc[r])], 1);
+    for (int t = ob + 32 * kOrderCached + lane; t < oe; t += 32)
         atomicAdd(&hist[key(count(t))], 1);
     __syncwarp();
     int const h = hist[lane];
@@ -730,18 +749,22 @@ __device__ void buildOwnerOrder(WarpMem<R> const& W, int words, int ob,
     __syncwarp();
     hist[lane] = incl - h;
     __syncwarp();
-    for (int t0 = ob; t0 < oe; t0 += 32)
-    {
+    auto place = [&](int t0, int c) {
         int const t = t0 + lane;
         bool const active = t < oe;
-        int const k = active ? key(count(t)) : 32 + lane;
+        int const k = active ? key(c) : 32 + lane;
         unsigned const peers = __match_any_sync(kFull, k);
         int const r = __popc(peers & ((1u << lane) - 1u));
         if (active) order[ob + hist[k] + r] = (unsigned short)t;
         __syncwarp();
         if (active && r == 0) hist[k] += __popc(peers);
         __syncwarp();
-    }
+    };
+#pragma unroll
+    for (int r = 0; r < kOrderCached; ++r)
+        if (ob + 32 * r < oe) place(ob + 32 * r, cc[r]);
+    for (int t0 = ob + 32 * kOrderCached; t0 < oe; t0 += 32)
+        place(t0, t0 + lane < oe ? count(t0 + lane) : 0);
 }
 
 // Rounds of 32 owners start at qBegin and advance by qStep (several warps
