@@ -80,9 +80,9 @@ STAGES = ("neighbor_list", "symmetry_functions", "neural_networks", "energy",
 # 24,576-atom frame by its neighbor entries (x 2.002): the staged-triplet
 # kernel (variants 6, 7; the default) and the per-owner kernel (0-5).
 SF_TRAFFIC = {
-    "staged": (2.520e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
+    "staged": (2.669e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
                         "the FP64 sfStagedKernel on the 12,288-atom box "
-                        "(1.259 GB), x 2.002 neighbor entries for 24,576 "
+                        "(1.333 GB), x 2.002 neighbor entries for 24,576 "
                         "atoms (profiles/sfStagedKernel_fp64_fp32_"
                         "water12288.md)"),
     "owner": (4.184e9, "ncu dram__bytes_read.sum + dram__bytes_write.sum of "
