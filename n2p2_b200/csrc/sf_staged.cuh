@@ -75,11 +75,14 @@ __host__ __device__ constexpr int stagedStride(int ns)
     return ns == 4 ? 21 : 3 + 3 * ns + kStagedRuns;
 }
 
-// Per-category constants of phase 1, shared by the warp's lanes.
+// Per-category constants of phase 1, shared by the warp's lanes; 16-byte
+// aligned fields, read in FP64 as pairs (lambda, zeta lambda), (eta, eta),
+// (a^2 / 4, -a^2 / 2) and quadruples of ints.
 template <typename R, int NS>
-struct StagedCat
+struct alignas(16) StagedCat
 {
-    R   lam[NS], zl[NS];
+    static_assert(NS % 4 == 0, "shapes in quadruples");
+    R   lz[2 * NS];          // lambda, zeta lambda of shape s at 2 s, 2 s + 1
     R   eta[kStagedRuns];
     int zi[NS];
     int eoff[kStagedRuns];   // offset of the run's exp table in W.E
@@ -224,9 +227,10 @@ __device__ __forceinline__ double expNonPositive(double x,
     p = fma(p, r, 0.5);
     double const q = fma(p, r2, r);
     double const tj = tab[k & (kExpTableSize - 1)];
-    int const m = k >> 6;
+    // m < -1022 gives two = +0 (the clamp to -1023 zeroes the exponent).
+    int const m = max(k >> 6, -1023);
     double const two = __hiloint2double((m + 1023) << 20, 0);
-    return m < -1022 ? 0.0 : fma(tj, q, tj) * two;
+    return fma(tj, q, tj) * two;
 }
 __device__ __forceinline__ float expNonPositive(float x, double const*)
 {
@@ -327,10 +331,11 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
     R pfcjk, qjk;
     if ((sizeof(R) == 8) && (CT == 1) && series)
     {
+        double2 const aq = *reinterpret_cast<double2 const*>(&C.a2q);
         double ch, sh;
-        halfAngleCosSinc((double)(C.a2q * r2), ch, sh);
+        halfAngleCosSinc(aq.x * (double)r2, ch, sh);
         pfcjk = R(ch * ch);
-        qjk = C.qf * R(sh * ch);
+        qjk = R(aq.y * (sh * ch));
     }
     else
     {
@@ -352,14 +357,37 @@ __device__ __forceinline__ void stagedRecord(SFParams const& P,
     rec[0] = dr2[0];
     rec[1] = dr2[1];
     rec[2] = dr2[2];
+    // The category's constants: pairs and quadruples in FP64.
+    int zis[NS];
+#pragma unroll
+    for (int q = 0; q < NS / 4; ++q)
+    {
+        int4 const v = reinterpret_cast<int4 const*>(C.zi)[q];
+        zis[4 * q] = v.x;
+        zis[4 * q + 1] = v.y;
+        zis[4 * q + 2] = v.z;
+        zis[4 * q + 3] = v.w;
+    }
 #pragma unroll
     for (int s = 0; s < NS; ++s)
     {
-        int const zi = C.zi[s];
-        R const pl = R(1) + C.lam[s] * cost;
+        R lam, zls;
+        if constexpr (sizeof(R) == 8)
+        {
+            double2 const v = reinterpret_cast<double2 const*>(C.lz)[s];
+            lam = v.x;
+            zls = v.y;
+        }
+        else
+        {
+            lam = C.lz[2 * s];
+            zls = C.lz[2 * s + 1];
+        }
+        int const zi = zis[s];
+        R const pl = R(1) + lam * cost;
         R const A = (pl <= R(0)) ? R(0) : powShape(pl, zi - 1);
         R const D = A * pl;
-        R const Azl = A * C.zl[s];
+        R const Azl = A * zls;
         rec[3 + 3 * s] = D * pfc;
         rec[4 + 3 * s] = Azl * Xc + D * pr13;
         rec[5 + 3 * s] = Azl * X3 - D * pr3;
@@ -406,8 +434,8 @@ __device__ void stagedNarrow(SFParams const& P, DevGroup const* G,
             for (int s = 0; s < NS; ++s)
             {
                 DevMember const& mm = M[g.mbeg + s];
-                cp->lam[s] = R(mm.lambda);
-                cp->zl[s] = R(mm.zetaLambda);
+                cp->lz[2 * s] = R(mm.lambda);
+                cp->lz[2 * s + 1] = R(mm.zetaLambda);
                 cp->zi[s] = mm.zetaInt;
             }
             for (int a = 0; a < kStagedRuns; ++a)
@@ -700,8 +728,8 @@ __device__ void stagedNarrowLock(SFParams const& P, DevGroup const* G,
         if (lane < NS)
         {
             DevMember const& mm = M[g.mbeg + lane];
-            cp->lam[lane] = R(mm.lambda);
-            cp->zl[lane] = R(mm.zetaLambda);
+            cp->lz[2 * lane] = R(mm.lambda);
+            cp->lz[2 * lane + 1] = R(mm.zetaLambda);
             cp->zi[lane] = mm.zetaInt;
         }
         else if (lane < NS + kStagedRuns)
